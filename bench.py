@@ -1,0 +1,325 @@
+"""Benchmark of the compressed product on B200.
+
+One step = one compressed product of a planted-entry workload: hash codes,
+per-k balancing, fused sketch/transform/accumulate, inverse, dense median
+decompression of all n_a x n_b entries into HBM, and device top-K recovery
+(K = planted count).  Default workload: n = 16384 square FP64, b = 2^16,
+d = 9, FFT variant, K = 256 (inputs 4.3 GB > L2, so no flush is needed).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--variant fft|fwht]
+                  [--workload config2_n16384|config2_n4096|config1]
+                  [--impl reference]
+
+--gpus N > 1 runs under torchrun, one rank per GPU, each rank an
+independent product (weak scaling, no collective on the data path; the
+path has none -- one product fits one GPU).  Prints one JSON line (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "compressed products/s"
+HBM_PEAK_FALLBACK = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="config2_n16384")
+    ap.add_argument("--variant", default="fft", choices=["fft", "fwht"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            m = json.load(f)
+        return float(m.get("hbm_gbs", HBM_PEAK_FALLBACK)), "measured"
+    return HBM_PEAK_FALLBACK, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks + throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def fft_flops(n_a, n_inner, n_b, d, b):
+    lb = np.log2(b)
+    return n_inner * d * (2 * 2.5 * b * lb + 8 * (b / 2 + 1) + 2 * (n_a + n_b)) + d * 2.5 * b * lb
+
+
+def fwht_ops(n_a, n_inner, n_b, d, b):
+    lb = np.log2(b)
+    return n_inner * d * (2 * b * lb + 2 * b + 2 * (n_a + n_b)) + d * b * lb
+
+
+# ------------------------------------------------------------- CPU legs
+def cpu_reference_sample(AT, B, n, d, b, variant, seed, budget_s):
+    """Time the reference's own CPU path (headers compiled with shims,
+    oracle/_ref) on a bounded sample and extrapolate to one product:
+    sketch over the first ks inner indices, decompression of the first
+    rows.  Returns (seconds_per_product, threads, sample description)."""
+    from oracle.oracle import RefLib
+    rl = RefLib()
+    thr = rl.num_threads()
+    ks = 8
+    while True:
+        t0 = time.perf_counter()
+        p = rl.compressed_product(variant, None, AT[:ks], B[:ks], d, b, seed)
+        ts = time.perf_counter() - t0
+        if ts > budget_s * 0.25 or ks >= n:
+            break
+        ks = min(n, ks * max(2, int(budget_s * 0.3 / max(ts, 1e-3))))
+    rows = 8
+    while True:
+        Cbuf = np.empty((rows, n))  # rows [0, rows) of C
+        t0 = time.perf_counter()
+        rl.decompress_rows(variant, None, p, d, b, seed, n, 0, rows, Cbuf)
+        tdec = time.perf_counter() - t0
+        if tdec > budget_s * 0.15 or rows >= n:
+            break
+        rows = min(n, rows * max(2, int(budget_s * 0.2 / max(tdec, 1e-3))))
+    per_product = ts * (n / ks) + tdec * (n / rows)
+    sample = (f"reference CPU path ({variant}) on the first {ks} of {n} inner indices "
+              f"({ts:.2f} s) and the first {rows} of {n} rows of the dense decompression "
+              f"({tdec:.2f} s), scaled linearly to one product")
+    return per_product, thr, sample
+
+
+# --------------------------------------------------------------- main
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from compmatmul_b200.planted import WORKLOADS, planted_problem
+    w = WORKLOADS[args.workload]
+    n, K, d, b = w["n"], w["K"], w["d"], w["b"]
+    variant = args.variant
+    config = {"workload": f"{args.workload}: planted-entry A,B {n}x{n} FP64 (noise N(0,0.01^2), "
+                          f"K={K} planted +10/+10), {variant.upper()}, b={b}, d={d}, "
+                          f"hash=multiply-add-shift; dense median decompression + top-{K}",
+              "n": n, "b": b, "d": d, "K": K, "variant": variant,
+              "l2": "inputs (2x8n^2 bytes) larger than L2, no flush"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        AT, B, _ = planted_problem(n, n, n, K, w["gen_seed"])
+        steps = []
+        thr, sample = 0, ""
+        for _ in range(max(1, args.steps)):
+            sec, thr, sample = cpu_reference_sample(AT, B, n, d, b, variant, w["seed"],
+                                                    args.cpu_seconds / max(1, args.steps) + 2)
+            steps.append(sec)
+        sec = float(np.median(steps))
+        val = 1.0 / sec
+        line = {"metric": METRIC, "value": val, "unit": "products/s", "impl": "reference",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": val, "unit": "products/s", "cores": thr,
+                                 "kind": "reference", "sample": sample},
+                "e2e": {"value": val, "unit": "products/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    import compmatmul_b200 as cmb
+    from compmatmul_b200 import device as dev
+
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    L = cmb.lib()
+    dv = torch.device("cuda", torch.cuda.current_device())
+
+    # inputs: per-rank seeds (independent products), pinned host + HBM copies
+    AT, B, planted = planted_problem(n, n, n, K, w["gen_seed"] + 1000 * rank)
+    hAT = torch.from_numpy(AT).pin_memory()
+    hB = torch.from_numpy(B).pin_memory()
+    dAT = hAT.to(dv)
+    dB = hB.to(dv)
+    dC = torch.empty((n, n), dtype=torch.float64, device=dv)
+    seed = w["seed"] + rank
+
+    def step():
+        dev.matmul(dAT, dB, d, b, seed, variant=variant, out=dC)
+        return dev.topk(dC, K, as_numpy=False)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    clocks = ClockSampler(torch.cuda.current_device())
+    L.cmm_profile_reset()
+    L.cmm_profile_enable(1)
+    launches0 = L.cmm_launch_count()
+    barrier()
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        out = step()
+    ev1.record()
+    barrier()
+    clk = clocks.stop()
+    launches = L.cmm_launch_count() - launches0
+    L.cmm_profile_enable(0)
+    total_ms = ev0.elapsed_time(ev1)
+    fam = {f: cmb.profile_read(f) for f in ("hash", "scale", "sketch", "finalize", "decompress", "topk")}
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dv)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * args.steps / (total_ms / 1e3)
+
+    # recovery check on this rank's last step (planted entries should be the top-K)
+    ti, tj, tv = [x.cpu().numpy() for x in out]
+    rec = len(set(zip(ti.tolist(), tj.tolist())) & set(zip(planted[0].tolist(), planted[2].tolist())))
+
+    # end to end through the C ABI with host (pinned) buffers
+    hC = torch.empty((n, n), dtype=torch.float64).pin_memory()
+    e2e_steps = max(1, args.e2e_steps)
+    import ctypes as C
+    for i in range(e2e_steps + 1):
+        if i == 1:
+            barrier()
+            te0 = time.perf_counter()
+        st = L.cmm_matmul(0 if variant == "fft" else 1, 1, n, n, n, C.c_void_p(hC.data_ptr()),
+                          C.c_void_p(hAT.data_ptr()), C.c_void_p(hB.data_ptr()), d, b, 1, seed)
+        cmb.check(st)
+    barrier()
+    e2e_s = (time.perf_counter() - te0) / e2e_steps
+    te = torch.tensor([e2e_s], dtype=torch.float64, device=dv)
+    if world > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = world / float(te.item())
+
+    # roofline of the dominant kernel (sketch)
+    sk_ms, sk_n = fam["sketch"]
+    sk_launch_ms = sk_ms / max(1, sk_n)
+    alg_bytes = 8.0 * n * (n + n)  # reads of AT and B per launch
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (sk_launch_ms / 1e3) / 1e9
+    flops = fft_flops(n, n, n, d, b) if variant == "fft" else fwht_ops(n, n, n, d, b)
+
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            sec, thr, sample = cpu_reference_sample(AT, B, n, d, b, variant, seed, args.cpu_seconds)
+            cpu = {"value": 1.0 / sec, "unit": "products/s", "cores": thr, "kind": "reference",
+                   "sample": sample}
+        except Exception as e:  # the checker binary may be absent
+            cpu = {"value": None, "unit": "products/s", "cores": 0, "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "products/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "kernel": "k_sketch_fft" if variant == "fft" else "k_sketch_fwht",
+                     "peak_source": peak_kind, "launch_ms": sk_launch_ms,
+                     "algorithmic_bytes_per_launch": alg_bytes,
+                     "fp64_tflops_achieved": flops / (sk_launch_ms / 1e3) / 1e12},
+        "kernel_ms_per_step": {k: v[0] / max(1, args.steps) for k, v in fam.items()},
+        "e2e": {"value": e2e_value, "unit": "products/s", "h2d_bytes_per_step": int(16 * n * n),
+                "d2h_bytes_per_step": int(8 * n * n)},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "recovered_planted": f"{rec}/{K}",
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

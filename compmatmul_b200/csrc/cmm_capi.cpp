@@ -1,0 +1,453 @@
+// Host runtime and C ABI of libcmm_b200.so (declared in
+// include/compmatmul_b200.h).  Validates arguments with the reference's
+// rules and messages (compmatmul.cpp:87-105), draws hash parameters on the
+// host (bit-exact with hashing.hpp), and runs the device pipeline:
+//   hash codes -> row balance (FFT) -> fused sketch/transform/accumulate
+//   -> k-group reduction + inverse -> (median decompression) -> (top-K).
+#include <cmath>
+#include <cstring>
+#include <atomic>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <utility>
+
+#include "../../include/compmatmul_b200.h"
+#include "cmm_internal.h"
+
+namespace cmm {
+
+static thread_local std::string g_last_error;
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    if (e == cudaErrorMemoryAllocation) throw std::bad_alloc();
+    throw cuda_error(std::string("CUDA error: ") + cudaGetErrorString(e) + " in " + what);
+  }
+}
+
+DevBuf::DevBuf(size_t n, cudaStream_t s) : bytes(n), stream(s) {
+  if (n) CMM_CUDA(cudaMallocAsync(&ptr, n, s));
+}
+DevBuf& DevBuf::operator=(DevBuf&& o) noexcept {
+  if (this != &o) {
+    if (ptr) cudaFreeAsync(ptr, stream);
+    ptr = o.ptr; bytes = o.bytes; stream = o.stream;
+    o.ptr = nullptr; o.bytes = 0;
+  }
+  return *this;
+}
+DevBuf::~DevBuf() {
+  if (ptr) cudaFreeAsync(ptr, stream);
+}
+
+int num_sms() {
+  static std::mutex mu;
+  static std::map<int, int> cache;
+  int dev = 0;
+  CMM_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  auto it = cache.find(dev);
+  if (it != cache.end()) return it->second;
+  int n = 0;
+  CMM_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+  cache[dev] = n;
+  return n;
+}
+
+// w[j] = exp(-2 pi i j / b), built in long double, cached per (device, b)
+const double2* twiddles(int b, cudaStream_t s) {
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, double2*> cache;
+  int dev = 0;
+  CMM_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  auto key = std::make_pair(dev, b);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  std::vector<double2> h((size_t)b);
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  for (int j = 0; j < b; ++j) {
+    const long double a = -two_pi * (long double)j / (long double)b;
+    h[(size_t)j] = make_double2((double)cosl(a), (double)sinl(a));
+  }
+  double2* d = nullptr;
+  CMM_CUDA(cudaMalloc(&d, sizeof(double2) * (size_t)b));
+  CMM_CUDA(cudaMemcpyAsync(d, h.data(), sizeof(double2) * (size_t)b, cudaMemcpyHostToDevice, s));
+  CMM_CUDA(cudaStreamSynchronize(s));
+  cache[key] = d;
+  return d;
+}
+
+// one non-blocking stream per (host thread, device) for the host-pointer API
+static cudaStream_t host_stream() {
+  static thread_local std::map<int, cudaStream_t> streams;
+  int dev = 0;
+  CMM_CUDA(cudaGetDevice(&dev));
+  auto it = streams.find(dev);
+  if (it != streams.end()) return it->second;
+  cudaStream_t s;
+  CMM_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  streams[dev] = s;
+  return s;
+}
+
+// --------------------------------------------------------------- checks
+static int ilog2_int(int b) {
+  int l = 0;
+  while ((1 << l) < b) ++l;
+  return l;
+}
+
+// compmatmul.cpp:87-105 (b, d, hash) plus this build's own limits
+static void check_params(int variant, int kind, int d, int b) {
+  if (variant != kVariantFFT && variant != kVariantFWHT)
+    throw invalid_argument("variant must be CMM_VARIANT_FFT or CMM_VARIANT_FWHT");
+  if (b < 2 || (b & (b - 1)) != 0)
+    throw invalid_argument("b must be power of 2 greater than 1 (got " + std::to_string(b) + ")");
+  if (d < 1) throw invalid_argument("d must be positive (got " + std::to_string(d) + ")");
+  if (kind < 0 || kind > 3)
+    throw invalid_argument(
+        "Invalid hash provided; hash must be one of `multiply shift', `multiply add shift', "
+        "`tabulation8', or `tabulation16'");
+  if (ilog2_int(b) > kMaxLog2B)
+    throw unsupported("b = " + std::to_string(b) + " exceeds the largest supported b (2^24)");
+  if (d > 65535) throw unsupported("d > 65535 is not supported");
+}
+
+static void check_sizes(int64_t n_a, int64_t n_inner, int64_t n_b) {
+  if (n_a < 0 || n_inner < 0 || n_b < 0) throw invalid_argument("negative matrix dimension");
+  if (n_a > 4294967296LL || n_b > 4294967296LL)
+    throw unsupported("matrix dimensions above 2^32 exceed the u32 hash key range");
+}
+
+// ------------------------------------------------------------- pipeline
+struct Codes {
+  DevBuf a, b;  // d x n_a, d x n_b
+};
+
+static DevBuf upload(const void* h, size_t n, cudaStream_t s) {
+  DevBuf d(n, s);
+  if (n) CMM_CUDA(cudaMemcpyAsync(d.ptr, h, n, cudaMemcpyHostToDevice, s));
+  return d;
+}
+
+// codes of both sides for keys 0..n_a-1 and 0..n_b-1
+static Codes make_codes(const SketchParams& sp, int64_t n_a, int64_t n_b, cudaStream_t s) {
+  DevBuf params = upload(sp.blob.data(), sp.blob.size(), s);
+  const size_t set = sp.fn_bytes * (size_t)sp.d;
+  const uint8_t* base = params.as<uint8_t>();
+  Codes c;
+  c.a = DevBuf((size_t)sp.d * (size_t)n_a * 4, s);
+  c.b = DevBuf((size_t)sp.d * (size_t)n_b * 4, s);
+  launch_hash_codes(sp.kind, base, base + 2 * set, sp.d, sp.log2b, n_a, c.a.as<uint32_t>(), s);
+  launch_hash_codes(sp.kind, base + set, base + 3 * set, sp.d, sp.log2b, n_b, c.b.as<uint32_t>(), s);
+  return c;
+}
+
+static void sketch_device(int variant, const SketchParams& sp, const Codes& codes, int64_t n_a,
+                          int64_t n_inner, int64_t n_b, const double* dAT, const double* dB,
+                          double* dP, cudaStream_t s) {
+  const SketchPlan P = plan_sketch(variant, n_a, n_inner, n_b, sp.d, sp.b, num_sms());
+  const double2* tw = twiddles(sp.b, s);
+  DevBuf scale;
+  if (variant == kVariantFFT) {
+    scale = DevBuf((size_t)(n_inner > 0 ? n_inner : 1) * 4, s);
+    launch_row_scale(dAT, dB, n_a, n_inner, n_b, scale.as<int>(), s);
+  }
+  const size_t elem = variant == kVariantFFT ? 16 : 8;
+  DevBuf partial((size_t)P.G * sp.d * (size_t)sp.b * elem, s);
+  launch_sketch_accumulate(P, dAT, dB, codes.a.as<uint32_t>(), codes.b.as<uint32_t>(),
+                           scale.as<int>(), tw, partial.ptr, s);
+  DevBuf work(2 * (size_t)sp.d * (size_t)sp.b * 16, s);
+  launch_finalize(P, partial.ptr, tw, work.ptr, dP, s);
+}
+
+static uint64_t pick_seed(int has_seed, uint64_t seed) { return has_seed ? seed : time_seed(); }
+
+// ------------------------------------------------------- instrumentation
+static std::atomic<int64_t> g_launches{0};
+static std::atomic<bool> g_prof{false};
+static std::mutex g_prof_mu;
+struct FamilyTimes {
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+  cudaEvent_t open = nullptr;
+};
+static std::map<std::string, FamilyTimes>& prof_table() {
+  static std::map<std::string, FamilyTimes> t;
+  return t;
+}
+
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+void prof_begin(const char* family, cudaStream_t s) {
+  if (!g_prof.load()) return;
+  std::lock_guard<std::mutex> g(g_prof_mu);
+  FamilyTimes& f = prof_table()[family];
+  cudaEvent_t e;
+  if (cudaEventCreate(&e) != cudaSuccess) return;
+  cudaEventRecord(e, s);
+  f.open = e;
+}
+
+void prof_end(const char* family, cudaStream_t s) {
+  if (!g_prof.load()) return;
+  std::lock_guard<std::mutex> g(g_prof_mu);
+  FamilyTimes& f = prof_table()[family];
+  if (!f.open) return;
+  cudaEvent_t e;
+  if (cudaEventCreate(&e) != cudaSuccess) return;
+  cudaEventRecord(e, s);
+  f.ev.emplace_back(f.open, e);
+  f.open = nullptr;
+}
+
+}  // namespace cmm
+
+// ================================================================= C ABI
+using namespace cmm;
+
+template <typename F>
+static int guarded(F&& f) {
+  try {
+    f();
+    g_last_error.clear();
+    return CMM_OK;
+  } catch (const cmm::invalid_argument& e) {
+    g_last_error = e.what();
+    return CMM_ERR_INVALID_ARGUMENT;
+  } catch (const cmm::unsupported& e) {
+    g_last_error = e.what();
+    return CMM_ERR_UNSUPPORTED;
+  } catch (const cmm::cuda_error& e) {
+    g_last_error = e.what();
+    return CMM_ERR_CUDA;
+  } catch (const std::bad_alloc&) {
+    g_last_error = "out of memory";
+    return CMM_ERR_NO_MEMORY;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return CMM_ERR_RUNTIME;
+  } catch (...) {
+    g_last_error = "unknown error";
+    return CMM_ERR_RUNTIME;
+  }
+}
+
+extern "C" {
+
+const char* cmm_last_error(void) { return g_last_error.c_str(); }
+
+const char* cmm_version(void) { return "compmatmul_b200 0.1.0 (sm_100a)"; }
+
+int cmm_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+int cmm_max_buckets(void) { return 1 << kMaxLog2B; }
+
+void cmm_profile_enable(int on) { g_prof.store(on != 0); }
+
+void cmm_profile_reset(void) {
+  std::lock_guard<std::mutex> g(g_prof_mu);
+  for (auto& kv : prof_table()) {
+    for (auto& pr : kv.second.ev) {
+      cudaEventSynchronize(pr.second);
+      cudaEventDestroy(pr.first);
+      cudaEventDestroy(pr.second);
+    }
+    if (kv.second.open) cudaEventDestroy(kv.second.open);
+  }
+  prof_table().clear();
+}
+
+int cmm_profile_read(const char* family, double* total_ms, int64_t* launches) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> g(g_prof_mu);
+    double tot = 0.0;
+    int64_t n = 0;
+    auto it = prof_table().find(family ? family : "");
+    if (it != prof_table().end()) {
+      for (auto& pr : it->second.ev) {
+        CMM_CUDA(cudaEventSynchronize(pr.second));
+        float ms = 0.f;
+        CMM_CUDA(cudaEventElapsedTime(&ms, pr.first, pr.second));
+        tot += ms;
+        ++n;
+      }
+    }
+    if (total_ms) *total_ms = tot;
+    if (launches) *launches = n;
+  });
+}
+
+int64_t cmm_launch_count(void) { return g_launches.load(); }
+
+int cmm_dev_compressed_product(int variant, int hash_kind, int64_t n_a, int64_t n_inner,
+                               int64_t n_b, const double* dAT, const double* dB, int d, int b,
+                               uint64_t seed, double* dP, void* stream) {
+  return guarded([&] {
+    check_params(variant, hash_kind, d, b);
+    check_sizes(n_a, n_inner, n_b);
+    cudaStream_t s = (cudaStream_t)stream;
+    SketchParams sp = make_sketch_params(hash_kind, d, b, seed);
+    Codes codes = make_codes(sp, n_a, n_b, s);
+    sketch_device(variant, sp, codes, n_a, n_inner, n_b, dAT, dB, dP, s);
+  });
+}
+
+int cmm_dev_decompress_dense(int variant, int hash_kind, int64_t n_a, int64_t n_b, int d, int b,
+                             uint64_t seed, const double* dP, double* dC, void* stream) {
+  return guarded([&] {
+    check_params(variant, hash_kind, d, b);
+    check_sizes(n_a, 0, n_b);
+    cudaStream_t s = (cudaStream_t)stream;
+    SketchParams sp = make_sketch_params(hash_kind, d, b, seed);
+    Codes codes = make_codes(sp, n_a, n_b, s);
+    launch_decompress_dense(variant, d, b, n_a, n_b, codes.a.as<uint32_t>(), codes.b.as<uint32_t>(),
+                            dP, dC, s);
+  });
+}
+
+int cmm_dev_matmul(int variant, int hash_kind, int64_t n_a, int64_t n_inner, int64_t n_b,
+                   double* dC, const double* dAT, const double* dB, int d, int b, uint64_t seed,
+                   void* stream) {
+  return guarded([&] {
+    check_params(variant, hash_kind, d, b);
+    check_sizes(n_a, n_inner, n_b);
+    cudaStream_t s = (cudaStream_t)stream;
+    SketchParams sp = make_sketch_params(hash_kind, d, b, seed);
+    Codes codes = make_codes(sp, n_a, n_b, s);
+    DevBuf P((size_t)d * (size_t)b * 8, s);
+    sketch_device(variant, sp, codes, n_a, n_inner, n_b, dAT, dB, P.as<double>(), s);
+    launch_decompress_dense(variant, d, b, n_a, n_b, codes.a.as<uint32_t>(), codes.b.as<uint32_t>(),
+                            P.as<double>(), dC, s);
+  });
+}
+
+int cmm_dev_topk(const double* dC, int64_t n_a, int64_t n_b, int K, uint32_t* d_i, uint32_t* d_j,
+                 double* d_v, void* stream) {
+  return guarded([&] {
+    if (n_a < 0 || n_b < 0 || K < 0) throw cmm::invalid_argument("negative size");
+    topk_dense(dC, n_a, n_b, K, d_i, d_j, d_v, (cudaStream_t)stream);
+  });
+}
+
+int cmm_dev_gemm(int64_t n_a, int64_t n_inner, int64_t n_b, double* dC, const double* dAT,
+                 const double* dB, void* stream) {
+  return guarded([&] {
+    check_sizes(n_a, n_inner, n_b);
+    launch_gemm(n_a, n_inner, n_b, dC, dAT, dB, (cudaStream_t)stream);
+  });
+}
+
+int cmm_compressed_product(int variant, int hash_kind, int64_t n_a, int64_t n_inner, int64_t n_b,
+                           const double* AT, const double* B, int d, int b, int has_seed,
+                           uint64_t seed, double* p_out, uint64_t* seed_out) {
+  return guarded([&] {
+    check_params(variant, hash_kind, d, b);
+    check_sizes(n_a, n_inner, n_b);
+    const uint64_t sd = pick_seed(has_seed, seed);
+    if (seed_out) *seed_out = sd;
+    cudaStream_t s = host_stream();
+    DevBuf dAT = upload(AT, (size_t)n_inner * n_a * 8, s);
+    DevBuf dB = upload(B, (size_t)n_inner * n_b * 8, s);
+    SketchParams sp = make_sketch_params(hash_kind, d, b, sd);
+    Codes codes = make_codes(sp, n_a, n_b, s);
+    DevBuf P((size_t)d * (size_t)b * 8, s);
+    sketch_device(variant, sp, codes, n_a, n_inner, n_b, dAT.as<double>(), dB.as<double>(),
+                  P.as<double>(), s);
+    CMM_CUDA(cudaMemcpyAsync(p_out, P.ptr, P.bytes, cudaMemcpyDeviceToHost, s));
+    CMM_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int cmm_matmul(int variant, int hash_kind, int64_t n_a, int64_t n_inner, int64_t n_b, double* C,
+               const double* AT, const double* B, int d, int b, int has_seed, uint64_t seed) {
+  return guarded([&] {
+    check_params(variant, hash_kind, d, b);
+    check_sizes(n_a, n_inner, n_b);
+    const uint64_t sd = pick_seed(has_seed, seed);
+    cudaStream_t s = host_stream();
+    DevBuf dAT = upload(AT, (size_t)n_inner * n_a * 8, s);
+    DevBuf dB = upload(B, (size_t)n_inner * n_b * 8, s);
+    DevBuf dC((size_t)n_a * n_b * 8, s);
+    SketchParams sp = make_sketch_params(hash_kind, d, b, sd);
+    Codes codes = make_codes(sp, n_a, n_b, s);
+    DevBuf P((size_t)d * (size_t)b * 8, s);
+    sketch_device(variant, sp, codes, n_a, n_inner, n_b, dAT.as<double>(), dB.as<double>(),
+                  P.as<double>(), s);
+    launch_decompress_dense(variant, d, b, n_a, n_b, codes.a.as<uint32_t>(), codes.b.as<uint32_t>(),
+                            P.as<double>(), dC.as<double>(), s);
+    if (dC.bytes) CMM_CUDA(cudaMemcpyAsync(C, dC.ptr, dC.bytes, cudaMemcpyDeviceToHost, s));
+    CMM_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int cmm_decompress(int variant, int hash_kind, int d, int b, uint64_t seed, const double* p,
+                   int64_t count, const uint32_t* i, const uint32_t* j, double* out) {
+  return guarded([&] {
+    check_params(variant, hash_kind, d, b);
+    if (count < 0) throw cmm::invalid_argument("negative count");
+    if (count == 0) return;
+    cudaStream_t s = host_stream();
+    SketchParams sp = make_sketch_params(hash_kind, d, b, seed);
+    DevBuf params = upload(sp.blob.data(), sp.blob.size(), s);
+    const size_t set = sp.fn_bytes * (size_t)d;
+    const uint8_t* base = params.as<uint8_t>();
+    DevBuf dI = upload(i, (size_t)count * 4, s), dJ = upload(j, (size_t)count * 4, s);
+    DevBuf cI((size_t)d * count * 4, s), cJ((size_t)d * count * 4, s);
+    launch_hash_codes_keys(hash_kind, base, base + 2 * set, d, sp.log2b, count, dI.as<uint32_t>(),
+                           cI.as<uint32_t>(), s);
+    launch_hash_codes_keys(hash_kind, base + set, base + 3 * set, d, sp.log2b, count,
+                           dJ.as<uint32_t>(), cJ.as<uint32_t>(), s);
+    DevBuf dP = upload(p, (size_t)d * b * 8, s);
+    DevBuf dOut((size_t)count * 8, s);
+    launch_decompress_list(variant, d, b, count, cI.as<uint32_t>(), cJ.as<uint32_t>(),
+                           dP.as<double>(), dOut.as<double>(), s);
+    CMM_CUDA(cudaMemcpyAsync(out, dOut.ptr, dOut.bytes, cudaMemcpyDeviceToHost, s));
+    CMM_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int cmm_gemm(int64_t n_a, int64_t n_inner, int64_t n_b, double* C, const double* AT,
+             const double* B) {
+  return guarded([&] {
+    check_sizes(n_a, n_inner, n_b);
+    cudaStream_t s = host_stream();
+    DevBuf dAT = upload(AT, (size_t)n_inner * n_a * 8, s);
+    DevBuf dB = upload(B, (size_t)n_inner * n_b * 8, s);
+    DevBuf dC((size_t)n_a * n_b * 8, s);
+    launch_gemm(n_a, n_inner, n_b, dC.as<double>(), dAT.as<double>(), dB.as<double>(), s);
+    if (dC.bytes) CMM_CUDA(cudaMemcpyAsync(C, dC.ptr, dC.bytes, cudaMemcpyDeviceToHost, s));
+    CMM_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int cmm_hash_codes(int hash_kind, int d, int b, uint64_t seed, int side, int64_t n,
+                   uint32_t* codes_out) {
+  return guarded([&] {
+    check_params(kVariantFFT, hash_kind, d, b);
+    if (side != 0 && side != 1) throw cmm::invalid_argument("side must be 0 or 1");
+    if (n < 0) throw cmm::invalid_argument("negative n");
+    if (n == 0) return;
+    cudaStream_t s = host_stream();
+    SketchParams sp = make_sketch_params(hash_kind, d, b, seed);
+    DevBuf params = upload(sp.blob.data(), sp.blob.size(), s);
+    const size_t set = sp.fn_bytes * (size_t)d;
+    const uint8_t* base = params.as<uint8_t>();
+    DevBuf c((size_t)d * n * 4, s);
+    launch_hash_codes(hash_kind, base + side * set, base + (2 + side) * set, d, sp.log2b, n,
+                      c.as<uint32_t>(), s);
+    CMM_CUDA(cudaMemcpyAsync(codes_out, c.ptr, c.bytes, cudaMemcpyDeviceToHost, s));
+    CMM_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+}  // extern "C"

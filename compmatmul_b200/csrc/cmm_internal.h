@@ -1,0 +1,155 @@
+// Internal declarations shared by the host runtime (cmm_capi.cu) and the
+// kernel translation units.  Not part of the public ABI.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+namespace cmm {
+
+// ------------------------------------------------------------------ errors
+// Exceptions thrown inside the runtime; the C ABI turns them into status
+// codes (compmatmul_b200.h).
+struct invalid_argument : std::invalid_argument {
+  using std::invalid_argument::invalid_argument;
+};
+struct runtime_error : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct unsupported : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct cuda_error : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+void cuda_check(cudaError_t e, const char* what);
+#define CMM_CUDA(call) ::cmm::cuda_check((call), #call)
+
+// ------------------------------------------------------- rng and hashing
+// xoshiro256** seeded by splitmix64 (rng.hpp:26-33, 59-72).
+struct Xoshiro256ss {
+  uint64_t s[4];
+  explicit Xoshiro256ss(uint64_t seed);
+  uint64_t operator()();
+};
+
+// Seed used when the caller gives none: rng()() with the ms clock seed
+// (rng.hpp:40-44, 54-56; matmul_fft.hpp:30-32).
+uint64_t time_seed();
+
+enum HashKind { MS = 0, MAS = 1, TAB8 = 2, TAB16 = 3 };
+
+size_t hash_param_bytes(int kind);
+
+// Parameters of `n` functions of family `kind` drawn from one stream
+// seeded with `seed` (hashing.hpp:69-87, 145-160, 277-295), packed as the
+// device kernels read them: MS -> n x u64 a; MAS -> n x (u64 a, u64 b);
+// TAB8 -> n x u32[4][256]; TAB16 -> n x u32[2][65536].
+std::vector<uint8_t> draw_hash_params(int kind, int n, uint64_t seed);
+
+// The four function sets of one sketch (matmul_sketch.hpp:15-18), each d
+// functions: order h1, h2, s1, s2.  One contiguous host blob.
+struct SketchParams {
+  int kind = 0, d = 0, b = 0, log2b = 0;
+  uint64_t seed = 0;
+  size_t fn_bytes = 0;  // bytes per function
+  std::vector<uint8_t> blob;  // [h1 | h2 | s1 | s2], each d * fn_bytes
+};
+SketchParams make_sketch_params(int kind, int d, int b, uint64_t seed);
+
+// ---------------------------------------------------------- device pool
+// Stream-ordered scratch allocation (cudaMallocAsync) with RAII release.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  cudaStream_t stream = nullptr;
+  DevBuf() = default;
+  DevBuf(size_t n, cudaStream_t s);
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept { *this = std::move(o); }
+  DevBuf& operator=(DevBuf&& o) noexcept;
+  ~DevBuf();
+  template <typename T>
+  T* as() const { return static_cast<T*>(ptr); }
+};
+
+// --------------------------------------------------------- kernel plans
+constexpr int kVariantFFT = 0;
+constexpr int kVariantFWHT = 1;
+
+// Largest sub-transform length held in one CTA's shared memory.
+constexpr int kFftLmaxLog = 12;   // 4096 complex FP64 (64 KB) + accumulator
+constexpr int kFwhtLmaxLog = 13;  // 8192 real FP64 x 2 (128 KB) + accumulator
+constexpr int kMaxLog2B = 24;     // b <= 2^24 (R = b/L <= 4096)
+
+struct SketchPlan {
+  int variant, d, b, log2b;
+  int logL, L;       // sub-transform length L = b / R
+  int logR, R;       // number of frequency slabs (CTAs) per repetition
+  int KB;            // sequences per CTA pass (KB * L = capacity)
+  int G;             // number of k groups
+  int64_t n_a, n_inner, n_b;
+};
+SketchPlan plan_sketch(int variant, int64_t n_a, int64_t n_inner, int64_t n_b, int d, int b,
+                       int num_sms);
+
+// Device-resident per-b twiddle table w[j] = exp(-2 pi i j / b), j < b
+// (double2), built on the host in long double and cached per (device, b).
+const double2* twiddles(int b, cudaStream_t s);
+
+// ------------------------------------------------------------- launchers
+void launch_hash_codes(int kind, const void* dHfns, const void* dSfns, int d, int log2b,
+                       int64_t n, uint32_t* dCodes, cudaStream_t s);
+// codes of explicit keys (dKeys[e]) instead of 0..n-1
+void launch_hash_codes_keys(int kind, const void* dHfns, const void* dSfns, int d, int log2b,
+                            int64_t n, const uint32_t* dKeys, uint32_t* dCodes, cudaStream_t s);
+
+void launch_row_scale(const double* dAT, const double* dB, int64_t n_a, int64_t n_inner,
+                      int64_t n_b, int* dScaleExp, cudaStream_t s);
+
+void launch_sketch_accumulate(const SketchPlan& P, const double* dAT, const double* dB,
+                              const uint32_t* dCodesA, const uint32_t* dCodesB,
+                              const int* dScaleExp, const double2* dTw, void* dPartial,
+                              cudaStream_t s);
+
+void launch_finalize(const SketchPlan& P, const void* dPartial, const double2* dTw,
+                     void* dWork, double* dP, cudaStream_t s);
+
+void launch_decompress_dense(int variant, int d, int b, int64_t n_a, int64_t n_b,
+                             const uint32_t* dCodesA, const uint32_t* dCodesB, const double* dP,
+                             double* dC, cudaStream_t s);
+
+// codes are d x count, one column per listed (i, j) entry
+void launch_decompress_list(int variant, int d, int b, int64_t count, const uint32_t* dCodesI,
+                            const uint32_t* dCodesJ, const double* dP, double* dOut,
+                            cudaStream_t s);
+
+void launch_gemm(int64_t n_a, int64_t n_inner, int64_t n_b, double* dC, const double* dAT,
+                 const double* dB, cudaStream_t s);
+
+// Top-K over a dense matrix; returns after synchronising s.
+void topk_dense(const double* dC, int64_t n_a, int64_t n_b, int K, uint32_t* dI, uint32_t* dJ,
+                double* dV, cudaStream_t s);
+
+int num_sms();
+
+// ------------------------------------------------------- instrumentation
+// Event timing of kernel families (cmm_profile_*) and the launch counter.
+void prof_begin(const char* family, cudaStream_t s);
+void prof_end(const char* family, cudaStream_t s);
+void count_launch(int n = 1);
+struct ProfScope {
+  const char* fam;
+  cudaStream_t s;
+  ProfScope(const char* f, cudaStream_t st) : fam(f), s(st) { prof_begin(fam, s); }
+  ~ProfScope() { prof_end(fam, s); }
+};
+
+}  // namespace cmm

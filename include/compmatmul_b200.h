@@ -1,0 +1,153 @@
+/*
+ * compmatmul_b200.h -- C ABI of the B200 (sm_100a) compressed matrix
+ * multiplication library (libcmm_b200.so).
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, and
+ * returns a cmm_status.  On failure cmm_last_error() gives the message
+ * (thread-local).  Status values map one-to-one onto the C++ exceptions of
+ * the reference binding: CMM_ERR_INVALID_ARGUMENT <-> std::invalid_argument
+ * (ValueError in Python), CMM_ERR_RUNTIME <-> std::runtime_error
+ * (RuntimeError), CMM_ERR_NO_MEMORY <-> std::bad_alloc (MemoryError).
+ *
+ * Conventions of the reference (matmul_fft.hpp:19-24, 149-154): AT is
+ * n_inner x n_a row-major, B is n_inner x n_b row-major, C = A^T... i.e.
+ * C[i][j] = sum_k AT[k][i] * B[k][j], n_a x n_b row-major.  The sketch p is
+ * d x b doubles (matmul_sketch::p, matmul_sketch.hpp:518).
+ *
+ * Hash kinds follow the strings of compmatmul.cpp:97-104.  Seeds follow
+ * matmul_sketch.hpp:15-18 (h1 <- seed, h2 <- seed+1, s1 <- seed+2,
+ * s2 <- seed+3).  has_seed == 0 draws the seed from the millisecond clock
+ * exactly as rng()() does (rng.hpp:54-56, matmul_fft.hpp:30-32).
+ *
+ * "host" entry points take host pointers, are synchronous, and allocate
+ * device memory internally (stream-ordered pool).  "dev" entry points take
+ * device pointers and a cudaStream_t (as void*), enqueue work on that
+ * stream and return without synchronising.
+ */
+#ifndef COMPMATMUL_B200_H
+#define COMPMATMUL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  CMM_OK = 0,
+  CMM_ERR_INVALID_ARGUMENT = 1, /* std::invalid_argument in the reference */
+  CMM_ERR_RUNTIME = 2,          /* std::runtime_error                    */
+  CMM_ERR_NO_MEMORY = 3,        /* std::bad_alloc                        */
+  CMM_ERR_CUDA = 4,             /* a CUDA call failed (no reference twin) */
+  CMM_ERR_UNSUPPORTED = 5       /* valid for the reference, beyond this build's limits */
+} cmm_status;
+
+typedef enum {
+  CMM_HASH_MULTIPLY_SHIFT = 0,     /* "multiply shift",     hashing.hpp:27-102  */
+  CMM_HASH_MULTIPLY_ADD_SHIFT = 1, /* "multiply add shift", hashing.hpp:111-183 (default) */
+  CMM_HASH_TABULATION8 = 2,        /* "tabulation8",        hashing.hpp:232-320 */
+  CMM_HASH_TABULATION16 = 3        /* "tabulation16",       hashing.hpp:232-320 */
+} cmm_hash_kind;
+
+typedef enum {
+  CMM_VARIANT_FFT = 0, /* cyclic convolution, matmul_fft.hpp  */
+  CMM_VARIANT_FWHT = 1 /* XOR convolution,     matmul_fwht.hpp */
+} cmm_variant;
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* cmm_last_error(void);
+/* Library version string. */
+const char* cmm_version(void);
+/* Number of CUDA devices visible (0 if none); never fails. */
+int cmm_device_count(void);
+
+/* Largest b the sketch kernels accept (2^24); larger powers of two give
+ * CMM_ERR_UNSUPPORTED. */
+int cmm_max_buckets(void);
+
+/* ---------------------------------------------------------------------
+ * Host-pointer drop-ins of the reference's header entry points.
+ * ------------------------------------------------------------------- */
+
+/* Replaces compmatmul::matmul_fft<H> (matmul_fft.hpp:155-178) and
+ * compmatmul::matmul_fwht<H> (matmul_fwht.hpp:144-167): compressed product
+ * followed by dense median decompression into C (n_a x n_b).  Argument
+ * checks of compmatmul.cpp:87-105 (b power of two > 1, d >= 1, hash). */
+int cmm_matmul(int variant, int hash_kind, int64_t n_a, int64_t n_inner, int64_t n_b, double* C,
+               const double* AT, const double* B, int d, int b, int has_seed, uint64_t seed);
+
+/* Replaces compmatmul::matmul_compressed_product_fft<H> (matmul_fft.hpp:25-129)
+ * and _fwht<H> (matmul_fwht.hpp:25-114): writes the d x b sketch p to p_out
+ * (host) and the seed actually used to *seed_out (may be NULL). */
+int cmm_compressed_product(int variant, int hash_kind, int64_t n_a, int64_t n_inner, int64_t n_b,
+                           const double* AT, const double* B, int d, int b, int has_seed,
+                           uint64_t seed, double* p_out, uint64_t* seed_out);
+
+/* Replaces compmatmul::matmul_decompress_fft<H> / _fwht<H>
+ * (matmul_fft.hpp:135-147, matmul_fwht.hpp:122-134) for `count` entries
+ * (i[e], j[e]): out[e] = median_t s1_t(i) s2_t(j) p_t[idx], idx = (h1+h2)&(b-1)
+ * (FFT) or h1^h2 (FWHT).  p is the host d x b sketch drawn with `seed`. */
+int cmm_decompress(int variant, int hash_kind, int d, int b, uint64_t seed, const double* p,
+                   int64_t count, const uint32_t* i, const uint32_t* j, double* out);
+
+/* Replaces compmatmul::array::matmul_gemm<double> (array.hpp:85-95) behind
+ * the Python `gemm` (compmatmul.cpp:76-85): exact C = AT^T B in FP64. */
+int cmm_gemm(int64_t n_a, int64_t n_inner, int64_t n_b, double* C, const double* AT,
+             const double* B);
+
+/* Bucket/sign codes of one side of the sketch for keys 0..n-1 (host
+ * output, d x n): code = bucket | (sign == +1) << 31; side 0 = (h1,s1),
+ * side 1 = (h2,s2).  Exposes hashing.hpp operator()/sign as computed on the
+ * GPU (the same codes the sketch kernels use). */
+int cmm_hash_codes(int hash_kind, int d, int b, uint64_t seed, int side, int64_t n,
+                   uint32_t* codes_out);
+
+/* ---------------------------------------------------------------------
+ * Device-pointer, stream-ordered entry points (no reference twin: the
+ * reference is host-only).  All pointers are device pointers.
+ * ------------------------------------------------------------------- */
+
+/* Sketch only: dP (d x b FP64) from dAT, dB. */
+int cmm_dev_compressed_product(int variant, int hash_kind, int64_t n_a, int64_t n_inner,
+                               int64_t n_b, const double* dAT, const double* dB, int d, int b,
+                               uint64_t seed, double* dP, void* stream);
+
+/* Dense median decompression of dP into dC (n_a x n_b FP64). */
+int cmm_dev_decompress_dense(int variant, int hash_kind, int64_t n_a, int64_t n_b, int d, int b,
+                             uint64_t seed, const double* dP, double* dC, void* stream);
+
+/* Compressed product + dense decompression (matmul_fft / matmul_fwht). */
+int cmm_dev_matmul(int variant, int hash_kind, int64_t n_a, int64_t n_inner, int64_t n_b,
+                   double* dC, const double* dAT, const double* dB, int d, int b, uint64_t seed,
+                   void* stream);
+
+/* Top-K entries of a dense n_a x n_b FP64 matrix on the device, by value
+ * descending, ties by (i, j) ascending.  Writes K (i, j, value) triples to
+ * device arrays.  Synchronises `stream` (the candidate count is read back). */
+int cmm_dev_topk(const double* dC, int64_t n_a, int64_t n_b, int K, uint32_t* d_i, uint32_t* d_j,
+                 double* d_v, void* stream);
+
+/* Exact FP64 C = AT^T B on the device. */
+int cmm_dev_gemm(int64_t n_a, int64_t n_inner, int64_t n_b, double* dC, const double* dAT,
+                 const double* dB, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Instrumentation for benchmarks (no reference twin).  When enabled, every
+ * kernel launch of a family is bracketed by CUDA events recorded on the
+ * stream it is launched on.  Families: "hash", "scale", "sketch",
+ * "finalize", "decompress", "topk", "gemm".
+ * ------------------------------------------------------------------- */
+void cmm_profile_enable(int on);
+void cmm_profile_reset(void);
+/* Sum of event-timed milliseconds and number of timed launches of a family
+ * since the last reset; waits for the recorded events. */
+int cmm_profile_read(const char* family, double* total_ms, int64_t* launches);
+/* Kernels launched by this library since load (always counted). */
+int64_t cmm_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* COMPMATMUL_B200_H */
