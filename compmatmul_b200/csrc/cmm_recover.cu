@@ -174,23 +174,30 @@ __device__ __forceinline__ uint64_t okey(double v) {
   return (b >> 63) ? ~b : (b | 0x8000000000000000ULL);
 }
 
-constexpr int kHistBits = 16;
+constexpr int kHistBits = 11;
 constexpr int kHistBins = 1 << kHistBits;
+constexpr int kLevels = 6;  // 5 x 11 bits + 9 bits = 64
 constexpr int kCandMax = 4096;
 
-// histogram of digit `level` (16 bits, level 0 = most significant) of the
-// keys whose higher digits equal `prefix`
+__host__ __device__ __forceinline__ int digit_bits(int level) {
+  return 64 - kHistBits * level < kHistBits ? 64 - kHistBits * level : kHistBits;
+}
+
+// histogram of digit `level` of the keys whose higher bits (the first
+// kHistBits * level) equal `prefix`
 __global__ void k_topk_hist(const double* __restrict__ C, int64_t n, int level, uint64_t prefix,
                             unsigned long long* __restrict__ hist) {
-  extern __shared__ unsigned int sh[];
+  __shared__ unsigned int sh[kHistBins];
   for (int i = threadIdx.x; i < kHistBins; i += blockDim.x) sh[i] = 0;
   __syncthreads();
-  const int shift = 64 - kHistBits * (level + 1);
-  const int pshift = 64 - kHistBits * level;  // bits above the digit
+  const int w = digit_bits(level);
+  const int pbits = kHistBits * level;
+  const int shift = 64 - pbits - w;
+  const uint64_t dmask = (1ULL << w) - 1ULL;
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n;
        idx += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t k = okey(__ldg(C + idx));
-    if (level == 0 || (k >> pshift) == prefix) atomicAdd(&sh[(k >> shift) & (kHistBins - 1)], 1u);
+    if (level == 0 || (k >> (64 - pbits)) == prefix) atomicAdd(&sh[(k >> shift) & dmask], 1u);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < kHistBins; i += blockDim.x)
@@ -199,11 +206,11 @@ __global__ void k_topk_hist(const double* __restrict__ C, int64_t n, int level, 
 
 // one thread: walk the histogram from the top and pick the digit where the
 // running count reaches `need`; out = {digit, count_above_in_level, count_in_bin}
-__global__ void k_topk_pick(const unsigned long long* __restrict__ hist, unsigned long long need,
-                            unsigned long long* __restrict__ out) {
+__global__ void k_topk_pick(const unsigned long long* __restrict__ hist, int nbins,
+                            unsigned long long need, unsigned long long* __restrict__ out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   unsigned long long run = 0;
-  for (int dgt = kHistBins - 1; dgt >= 0; --dgt) {
+  for (int dgt = nbins - 1; dgt >= 0; --dgt) {
     const unsigned long long c = hist[dgt];
     if (run + c >= need) {
       out[0] = (unsigned long long)dgt;
@@ -330,31 +337,31 @@ void topk_dense(const double* dC, int64_t n_a, int64_t n_b, int K, uint32_t* dI,
   DevBuf keys((size_t)kCandMax * 8, s), idxs((size_t)kCandMax * 8, s), cnt(8, s);
   int64_t blocks = (n + 255) / 256;
   if (blocks > 4 * num_sms()) blocks = 4 * num_sms();
-  const int hsmem = kHistBins * 4;
-  CMM_CUDA(cudaFuncSetAttribute(k_topk_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, hsmem));
   uint64_t prefix = 0;              // selected digits so far
   unsigned long long need = (unsigned long long)K;  // still to take at this prefix
   unsigned long long above = 0;     // taken strictly above the prefix (all levels)
   int level = 0;
+  int pbits = 0;
   unsigned long long h_pick[3];
   bool tie = false;
-  for (; level < 4; ++level) {
+  for (; level < kLevels; ++level) {
+    const int w = digit_bits(level);
     CMM_CUDA(cudaMemsetAsync(hist.ptr, 0, hist.bytes, s));
     count_launch(2);
-    k_topk_hist<<<(unsigned)blocks, 256, hsmem, s>>>(dC, n, level, prefix, hist.as<unsigned long long>());
+    k_topk_hist<<<(unsigned)blocks, 256, 0, s>>>(dC, n, level, prefix, hist.as<unsigned long long>());
     CMM_CUDA(cudaGetLastError());
-    k_topk_pick<<<1, 32, 0, s>>>(hist.as<unsigned long long>(), need, pick.as<unsigned long long>());
+    k_topk_pick<<<1, 32, 0, s>>>(hist.as<unsigned long long>(), 1 << w, need,
+                                 pick.as<unsigned long long>());
     CMM_CUDA(cudaMemcpyAsync(h_pick, pick.ptr, sizeof(h_pick), cudaMemcpyDeviceToHost, s));
     CMM_CUDA(cudaStreamSynchronize(s));
-    prefix = (prefix << kHistBits) | h_pick[0];
+    prefix = (prefix << w) | h_pick[0];
+    pbits += w;
     above += h_pick[1];
     need -= h_pick[1];
     // everything at this prefix fits: collect >= prefix and sort
     if (above + h_pick[2] <= (unsigned long long)kCandMax) break;
-    if (level == 3) tie = true;  // > kCandMax entries share the K-th key exactly
+    if (level == kLevels - 1) tie = true;  // > kCandMax entries share the K-th key exactly
   }
-  if (level > 3) level = 3;
-  const int pbits = kHistBits * (level + 1);
   CMM_CUDA(cudaMemsetAsync(cnt.ptr, 0, 8, s));
   count_launch(tie ? 4 : 2);
   if (!tie) {
