@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--n", type=int, default=0, help="override the workload size (profiling)")
     return ap.parse_args()
 
 
@@ -160,7 +161,9 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     from compmatmul_b200.planted import WORKLOADS, planted_problem
-    w = WORKLOADS[args.workload]
+    w = dict(WORKLOADS[args.workload])
+    if args.n:
+        w["n"] = args.n
     n, K, d, b = w["n"], w["K"], w["d"], w["b"]
     variant = args.variant
     config = {"workload": f"{args.workload}: planted-entry A,B {n}x{n} FP64 (noise N(0,0.01^2), "

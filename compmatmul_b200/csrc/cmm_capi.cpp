@@ -27,8 +27,13 @@ void cuda_check(cudaError_t e, const char* what) {
   }
 }
 
+static void configure_pool();
+
 DevBuf::DevBuf(size_t n, cudaStream_t s) : bytes(n), stream(s) {
-  if (n) CMM_CUDA(cudaMallocAsync(&ptr, n, s));
+  if (n) {
+    configure_pool();
+    CMM_CUDA(cudaMallocAsync(&ptr, n, s));
+  }
 }
 DevBuf& DevBuf::operator=(DevBuf&& o) noexcept {
   if (this != &o) {
@@ -78,6 +83,23 @@ const double2* twiddles(int b, cudaStream_t s) {
   CMM_CUDA(cudaStreamSynchronize(s));
   cache[key] = d;
   return d;
+}
+
+// Keep freed blocks of the device's default stream-ordered pool cached
+// (release threshold = max) so repeated calls do not re-map GBs of device
+// memory at every synchronisation.  Once per device.
+static void configure_pool() {
+  static std::mutex mu;
+  static std::map<int, bool> done;
+  int dev = 0;
+  CMM_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  if (done[dev]) return;
+  cudaMemPool_t pool;
+  CMM_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+  uint64_t thr = ~0ULL;
+  CMM_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+  done[dev] = true;
 }
 
 // one non-blocking stream per (host thread, device) for the host-pointer API
@@ -146,17 +168,47 @@ static Codes make_codes(const SketchParams& sp, int64_t n_a, int64_t n_b, cudaSt
   return c;
 }
 
+// Budget for the per-chunk materialized rows (d copies of each row pair).
+static size_t materialize_budget() {
+  size_t free_b = 0, total_b = 0;
+  CMM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  size_t cap = (size_t)8 << 30;
+  return free_b / 3 < cap ? free_b / 3 : cap;
+}
+
 static void sketch_device(int variant, const SketchParams& sp, const Codes& codes, int64_t n_a,
                           int64_t n_inner, int64_t n_b, const double* dAT, const double* dB,
                           double* dP, cudaStream_t s) {
-  const SketchPlan P = plan_sketch(variant, n_a, n_inner, n_b, sp.d, sp.b, num_sms());
   const double2* tw = twiddles(sp.b, s);
+  const size_t elem = variant == kVariantFFT ? 16 : 8;
   DevBuf scale;
   if (variant == kVariantFFT) {
     scale = DevBuf((size_t)(n_inner > 0 ? n_inner : 1) * 4, s);
     launch_row_scale(dAT, dB, n_a, n_inner, n_b, scale.as<int>(), s);
   }
-  const size_t elem = variant == kVariantFFT ? 16 : 8;
+  if (n_inner > 0 && sketch_v1_applicable(variant, sp.b, n_a, n_b)) {
+    // bucket-sorted plan + per-chunk materialized rows + v1 kernels
+    const SketchPlan P = plan_sketch_v1(variant, n_a, n_inner, n_b, sp.d, sp.b, num_sms());
+    SlabPlan plan = make_slab_plan(codes.a.as<uint32_t>(), codes.b.as<uint32_t>(), n_a, n_b, sp.d,
+                                   sp.b, P.logL, s);
+    const int64_t SA = (int64_t)plan.EA * kPlanThreads, SB = (int64_t)plan.EB * kPlanThreads;
+    const size_t per_row = (size_t)sp.d * (size_t)(SA + SB) * 8;
+    int64_t kc = (int64_t)(materialize_budget() / per_row);
+    if (kc < 1) kc = 1;
+    if (kc > n_inner) kc = n_inner;
+    DevBuf matA((size_t)sp.d * kc * SA * 8, s), matB((size_t)sp.d * kc * SB * 8, s);
+    DevBuf partial((size_t)P.G * sp.d * (size_t)sp.b * elem, s);
+    for (int64_t k0 = 0; k0 < n_inner; k0 += kc) {
+      const int64_t c = n_inner - k0 < kc ? n_inner - k0 : kc;
+      launch_materialize(plan, dAT, dB, k0, c, matA.as<double>(), matB.as<double>(), s);
+      launch_sketch_v1(P, plan, matA.as<double>(), matB.as<double>(), c, scale.as<int>(), k0, tw,
+                       partial.ptr, k0 > 0 ? 1 : 0, s);
+    }
+    DevBuf work(2 * (size_t)sp.d * (size_t)sp.b * 16, s);
+    launch_finalize(P, partial.ptr, tw, work.ptr, dP, s);
+    return;
+  }
+  const SketchPlan P = plan_sketch(variant, n_a, n_inner, n_b, sp.d, sp.b, num_sms());
   DevBuf partial((size_t)P.G * sp.d * (size_t)sp.b * elem, s);
   launch_sketch_accumulate(P, dAT, dB, codes.a.as<uint32_t>(), codes.b.as<uint32_t>(),
                            scale.as<int>(), tw, partial.ptr, s);

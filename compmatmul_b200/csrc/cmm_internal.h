@@ -134,6 +134,33 @@ void launch_decompress_list(int variant, int d, int b, int64_t count, const uint
 void launch_gemm(int64_t n_a, int64_t n_inner, int64_t n_b, double* dC, const double* dAT,
                  const double* dB, cudaStream_t s);
 
+// ---------------------------------------------------------- slab plans
+// Bucket-sorted, thread-interleaved slot layout of one sketch (see
+// cmm_plan.cu) and its per-t materialized rows (sketch kernels v1).
+constexpr int kPlanThreads = 512;          // threads of the v1 sketch kernels
+constexpr uint32_t kPadSlot = 0xffffffffu;  // slot without an index
+struct SlabPlan {
+  int d = 0, logL = 0, EA = 0, EB = 0;
+  bool u16 = true;  // codes stored as u16 (b <= 2^16)
+  int64_t n_a = 0, n_b = 0;
+  DevBuf srcA, srcB;      // d x S: index | (sign == +1) << 31, or kPadSlot
+  DevBuf codeA, codeB;    // d x S: bucket h
+  DevBuf countA, countB;  // d x kPlanThreads: slots used per thread
+};
+SlabPlan make_slab_plan(const uint32_t* dCodesA, const uint32_t* dCodesB, int64_t n_a, int64_t n_b,
+                        int d, int b, int logL, cudaStream_t s);
+void launch_materialize(const SlabPlan& P, const double* dAT, const double* dB, int64_t k0,
+                        int64_t kc, double* dOutA, double* dOutB, cudaStream_t s);
+// v1 sketch over materialized rows of inner indices [k0, k0 + kc) (chunk);
+// accumulate != 0 adds to the partials instead of overwriting them.
+void launch_sketch_v1(const SketchPlan& SP, const SlabPlan& P, const double* dMatA,
+                      const double* dMatB, int64_t kc, const int* dScaleExp, int64_t k0,
+                      const double2* dTw, void* dPartial, int accumulate, cudaStream_t s);
+SketchPlan plan_sketch_v1(int variant, int64_t n_a, int64_t n_inner, int64_t n_b, int d, int b,
+                          int sms);
+// true if the v1 kernels handle this (variant, b, n) and sizes
+bool sketch_v1_applicable(int variant, int b, int64_t n_a, int64_t n_b);
+
 // Top-K over a dense matrix; returns after synchronising s.
 void topk_dense(const double* dC, int64_t n_a, int64_t n_b, int K, uint32_t* dI, uint32_t* dJ,
                 double* dV, cudaStream_t s);

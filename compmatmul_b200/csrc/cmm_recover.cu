@@ -197,7 +197,14 @@ __global__ void k_topk_hist(const double* __restrict__ C, int64_t n, int level, 
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n;
        idx += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t k = okey(__ldg(C + idx));
-    if (level == 0 || (k >> (64 - pbits)) == prefix) atomicAdd(&sh[(k >> shift) & dmask], 1u);
+    const bool in = level == 0 || (k >> (64 - pbits)) == prefix;
+    // warp-aggregated: one shared atomic per distinct digit in the warp
+    // (values cluster in few digits, plain atomics would serialise)
+    const uint32_t dg = in ? (uint32_t)((k >> shift) & dmask) : 0xffffffffu;
+    const uint32_t active = __activemask();
+    const uint32_t peers = __match_any_sync(active, dg);
+    const int lane = threadIdx.x & 31;
+    if (in && lane == __ffs(peers) - 1) atomicAdd(&sh[dg], (unsigned)__popc(peers));
   }
   __syncthreads();
   for (int i = threadIdx.x; i < kHistBins; i += blockDim.x)

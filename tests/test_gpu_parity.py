@@ -95,16 +95,22 @@ def test_fft_unbalanced_row_scales(gpu, oracle):
     np.testing.assert_allclose(p_gpu, p_ref, rtol=0, atol=p_tol(p_ref))
 
 
-def test_zero_and_empty_inner(gpu, oracle):
+@pytest.mark.parametrize("b", [64, 8192])
+def test_zero_and_empty_inner(gpu, oracle, b):
     AT = np.zeros((5, 8))
     B = np.ones((5, 9))
     for v in ("fft", "fwht"):
-        p, _ = capi().compressed_product(v, None, AT, B, 3, 64, 1)
-        assert np.array_equal(p, np.zeros((3, 64)))
-        p0, _ = capi().compressed_product(v, None, np.zeros((0, 8)), np.zeros((0, 9)), 3, 64, 1)
-        assert np.array_equal(p0, np.zeros((3, 64)))
-        C = capi().matmul(v, None, np.zeros((0, 8)), np.zeros((0, 9)), 3, 64, 1)
+        p, _ = capi().compressed_product(v, None, AT, B, 3, b, 1)
+        assert np.array_equal(p, np.zeros((3, b)))
+        p0, _ = capi().compressed_product(v, None, np.zeros((0, 8)), np.zeros((0, 9)), 3, b, 1)
+        assert np.array_equal(p0, np.zeros((3, b)))
+        C = capi().matmul(v, None, np.zeros((0, 8)), np.zeros((0, 9)), 3, b, 1)
         assert np.array_equal(C, np.zeros((8, 9)))
+        # one side empty (n_a = 0 / n_b = 0)
+        pa, _ = capi().compressed_product(v, None, np.ones((4, 0)), np.ones((4, 6)), 2, b, 3)
+        assert np.array_equal(pa, np.zeros((2, b)))
+        pb, _ = capi().compressed_product(v, None, np.ones((4, 6)), np.ones((4, 0)), 2, b, 3)
+        assert np.array_equal(pb, np.zeros((2, b)))
 
 
 # ----------------------------------------------------------- dense matmul
