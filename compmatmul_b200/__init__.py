@@ -34,7 +34,8 @@ EXPORTED = [
     "cmm_compressed_product", "cmm_decompress", "cmm_gemm", "cmm_hash_codes",
     "cmm_dev_compressed_product", "cmm_dev_decompress_dense", "cmm_dev_matmul", "cmm_dev_topk",
     "cmm_dev_gemm", "cmm_profile_enable", "cmm_profile_reset", "cmm_profile_read",
-    "cmm_launch_count",
+    "cmm_launch_count", "cmm_dev_compressed_product_f32", "cmm_dev_matmul_f32",
+    "cmm_compressed_product_f32", "cmm_matmul_f32",
 ]
 
 
@@ -73,6 +74,10 @@ def lib():
     L.cmm_dev_matmul.argtypes = [i32, i32, i64, i64, i64, dp, dp, dp, i32, i32, u64, vp]
     L.cmm_dev_topk.argtypes = [dp, i64, i64, i32, vp, vp, dp, vp]
     L.cmm_dev_gemm.argtypes = [i64, i64, i64, dp, dp, dp, vp]
+    L.cmm_dev_compressed_product_f32.argtypes = [i32, i32, i64, i64, i64, dp, dp, i32, i32, u64, dp, vp]
+    L.cmm_dev_matmul_f32.argtypes = [i32, i32, i64, i64, i64, dp, dp, dp, i32, i32, u64, vp]
+    L.cmm_compressed_product_f32.argtypes = [i32, i32, i64, i64, i64, dp, dp, i32, i32, i32, u64, dp, vp]
+    L.cmm_matmul_f32.argtypes = [i32, i32, i64, i64, i64, dp, dp, dp, i32, i32, i32, u64]
     L.cmm_profile_enable.argtypes = [i32]
     L.cmm_profile_enable.restype = None
     L.cmm_profile_reset.restype = None

@@ -80,3 +80,29 @@ def gemm(AT, B):
     Cm = np.empty((n_a, n_b))
     check(lib().cmm_gemm(n_a, q, n_b, _p(Cm), _p(AT), _p(B)))
     return Cm
+
+
+def compressed_product_f32(variant, hash_name, AT, B, d, b, seed=None):
+    """Mixed precision sketch from FP32 inputs; p is FP64 (d x b)."""
+    AT = np.ascontiguousarray(AT, dtype=np.float32)
+    B = np.ascontiguousarray(B, dtype=np.float32)
+    q, n_a = AT.shape
+    n_b = B.shape[1]
+    p = np.empty((d, b))
+    used = C.c_uint64(0)
+    check(lib().cmm_compressed_product_f32(_var(variant), _kind(hash_name), n_a, q, n_b, _p(AT),
+                                           _p(B), d, b, 0 if seed is None else 1,
+                                           0 if seed is None else seed, _p(p), C.byref(used)))
+    return p, used.value
+
+
+def matmul_f32(variant, hash_name, AT, B, d, b, seed=None):
+    """Mixed precision dense estimate (FP64 output) from FP32 inputs."""
+    AT = np.ascontiguousarray(AT, dtype=np.float32)
+    B = np.ascontiguousarray(B, dtype=np.float32)
+    q, n_a = AT.shape
+    n_b = B.shape[1]
+    Cm = np.empty((n_a, n_b))
+    check(lib().cmm_matmul_f32(_var(variant), _kind(hash_name), n_a, q, n_b, _p(Cm), _p(AT), _p(B),
+                               d, b, 0 if seed is None else 1, 0 if seed is None else seed))
+    return Cm

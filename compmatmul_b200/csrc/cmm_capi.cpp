@@ -216,6 +216,43 @@ static void sketch_device(int variant, const SketchParams& sp, const Codes& code
   launch_finalize(P, partial.ptr, tw, work.ptr, dP, s);
 }
 
+// Mixed-precision compressed product from FP32 inputs.  Slabs of 8192 on
+// the FP32 kernels when b >= 8192; smaller b runs the FP64 kernels on an
+// FP64 copy of the inputs (on the device).
+static void sketch_device_mixed(int variant, const SketchParams& sp, const Codes& codes,
+                                int64_t n_a, int64_t n_inner, int64_t n_b, const float* dAT,
+                                const float* dB, double* dP, cudaStream_t s) {
+  if (!(n_inner > 0 && sketch_mixed_applicable(variant, sp.b))) {
+    DevBuf A64((size_t)n_inner * n_a * 8, s), B64((size_t)n_inner * n_b * 8, s);
+    launch_f32_to_f64(dAT, A64.as<double>(), n_inner * n_a, s);
+    launch_f32_to_f64(dB, B64.as<double>(), n_inner * n_b, s);
+    sketch_device(variant, sp, codes, n_a, n_inner, n_b, A64.as<double>(), B64.as<double>(), dP, s);
+    return;
+  }
+  const double2* tw = twiddles(sp.b, s);
+  const size_t elem = variant == kVariantFFT ? 16 : 8;
+  DevBuf scale((size_t)n_inner * 4, s);
+  if (variant == kVariantFFT) launch_row_scale_f32(dAT, dB, n_a, n_inner, n_b, scale.as<int>(), s);
+  const SketchPlan P = plan_sketch_mixed(variant, n_a, n_inner, n_b, sp.d, sp.b, num_sms());
+  SlabPlan plan = make_slab_plan(codes.a.as<uint32_t>(), codes.b.as<uint32_t>(), n_a, n_b, sp.d,
+                                 sp.b, P.logL, s);
+  const int64_t SA = (int64_t)plan.EA * kPlanThreads, SB = (int64_t)plan.EB * kPlanThreads;
+  const size_t per_row = (size_t)sp.d * (size_t)(SA + SB) * 4;
+  int64_t kc = (int64_t)(materialize_budget() / per_row);
+  if (kc < 1) kc = 1;
+  if (kc > n_inner) kc = n_inner;
+  DevBuf matA((size_t)sp.d * kc * SA * 4, s), matB((size_t)sp.d * kc * SB * 4, s);
+  DevBuf partial((size_t)P.G * sp.d * (size_t)sp.b * elem, s);
+  for (int64_t k0 = 0; k0 < n_inner; k0 += kc) {
+    const int64_t c = n_inner - k0 < kc ? n_inner - k0 : kc;
+    launch_materialize_f32(plan, dAT, dB, k0, c, matA.as<float>(), matB.as<float>(), s);
+    launch_sketch_mixed(P, plan, matA.as<float>(), matB.as<float>(), c, scale.as<int>(), k0, tw,
+                        partial.ptr, k0 > 0 ? 1 : 0, s);
+  }
+  DevBuf work(2 * (size_t)sp.d * (size_t)sp.b * 16, s);
+  launch_finalize(P, partial.ptr, tw, work.ptr, dP, s);
+}
+
 static uint64_t pick_seed(int has_seed, uint64_t seed) { return has_seed ? seed : time_seed(); }
 
 // ------------------------------------------------------- instrumentation
@@ -396,6 +433,79 @@ int cmm_dev_gemm(int64_t n_a, int64_t n_inner, int64_t n_b, double* dC, const do
   return guarded([&] {
     check_sizes(n_a, n_inner, n_b);
     launch_gemm(n_a, n_inner, n_b, dC, dAT, dB, (cudaStream_t)stream);
+  });
+}
+
+int cmm_dev_compressed_product_f32(int variant, int hash_kind, int64_t n_a, int64_t n_inner,
+                                   int64_t n_b, const float* dAT, const float* dB, int d, int b,
+                                   uint64_t seed, double* dP, void* stream) {
+  return guarded([&] {
+    check_params(variant, hash_kind, d, b);
+    check_sizes(n_a, n_inner, n_b);
+    cudaStream_t s = (cudaStream_t)stream;
+    SketchParams sp = make_sketch_params(hash_kind, d, b, seed);
+    Codes codes = make_codes(sp, n_a, n_b, s);
+    sketch_device_mixed(variant, sp, codes, n_a, n_inner, n_b, dAT, dB, dP, s);
+  });
+}
+
+int cmm_dev_matmul_f32(int variant, int hash_kind, int64_t n_a, int64_t n_inner, int64_t n_b,
+                       double* dC, const float* dAT, const float* dB, int d, int b, uint64_t seed,
+                       void* stream) {
+  return guarded([&] {
+    check_params(variant, hash_kind, d, b);
+    check_sizes(n_a, n_inner, n_b);
+    cudaStream_t s = (cudaStream_t)stream;
+    SketchParams sp = make_sketch_params(hash_kind, d, b, seed);
+    Codes codes = make_codes(sp, n_a, n_b, s);
+    DevBuf P((size_t)d * (size_t)b * 8, s);
+    sketch_device_mixed(variant, sp, codes, n_a, n_inner, n_b, dAT, dB, P.as<double>(), s);
+    launch_decompress_dense(variant, d, b, n_a, n_b, codes.a.as<uint32_t>(), codes.b.as<uint32_t>(),
+                            P.as<double>(), dC, s);
+  });
+}
+
+int cmm_compressed_product_f32(int variant, int hash_kind, int64_t n_a, int64_t n_inner,
+                               int64_t n_b, const float* AT, const float* B, int d, int b,
+                               int has_seed, uint64_t seed, double* p_out, uint64_t* seed_out) {
+  return guarded([&] {
+    check_params(variant, hash_kind, d, b);
+    check_sizes(n_a, n_inner, n_b);
+    const uint64_t sd = pick_seed(has_seed, seed);
+    if (seed_out) *seed_out = sd;
+    cudaStream_t s = host_stream();
+    DevBuf dAT = upload(AT, (size_t)n_inner * n_a * 4, s);
+    DevBuf dB = upload(B, (size_t)n_inner * n_b * 4, s);
+    SketchParams sp = make_sketch_params(hash_kind, d, b, sd);
+    Codes codes = make_codes(sp, n_a, n_b, s);
+    DevBuf P((size_t)d * (size_t)b * 8, s);
+    sketch_device_mixed(variant, sp, codes, n_a, n_inner, n_b, dAT.as<float>(), dB.as<float>(),
+                        P.as<double>(), s);
+    CMM_CUDA(cudaMemcpyAsync(p_out, P.ptr, P.bytes, cudaMemcpyDeviceToHost, s));
+    CMM_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int cmm_matmul_f32(int variant, int hash_kind, int64_t n_a, int64_t n_inner, int64_t n_b,
+                   double* C, const float* AT, const float* B, int d, int b, int has_seed,
+                   uint64_t seed) {
+  return guarded([&] {
+    check_params(variant, hash_kind, d, b);
+    check_sizes(n_a, n_inner, n_b);
+    const uint64_t sd = pick_seed(has_seed, seed);
+    cudaStream_t s = host_stream();
+    DevBuf dAT = upload(AT, (size_t)n_inner * n_a * 4, s);
+    DevBuf dB = upload(B, (size_t)n_inner * n_b * 4, s);
+    DevBuf dC((size_t)n_a * n_b * 8, s);
+    SketchParams sp = make_sketch_params(hash_kind, d, b, sd);
+    Codes codes = make_codes(sp, n_a, n_b, s);
+    DevBuf P((size_t)d * (size_t)b * 8, s);
+    sketch_device_mixed(variant, sp, codes, n_a, n_inner, n_b, dAT.as<float>(), dB.as<float>(),
+                        P.as<double>(), s);
+    launch_decompress_dense(variant, d, b, n_a, n_b, codes.a.as<uint32_t>(), codes.b.as<uint32_t>(),
+                            P.as<double>(), dC.as<double>(), s);
+    if (dC.bytes) CMM_CUDA(cudaMemcpyAsync(C, dC.ptr, dC.bytes, cudaMemcpyDeviceToHost, s));
+    CMM_CUDA(cudaStreamSynchronize(s));
   });
 }
 

@@ -161,6 +161,20 @@ SketchPlan plan_sketch_v1(int variant, int64_t n_a, int64_t n_inner, int64_t n_b
 // true if the v1 kernels handle this (variant, b, n) and sizes
 bool sketch_v1_applicable(int variant, int b, int64_t n_a, int64_t n_b);
 
+// Mixed precision (FP32 inputs, FP32 transforms, compensated accumulation,
+// FP64 reduction and inverse): slabs of L = 8192 (cmm_sketch_mixed.cu).
+SketchPlan plan_sketch_mixed(int variant, int64_t n_a, int64_t n_inner, int64_t n_b, int d, int b,
+                             int sms);
+bool sketch_mixed_applicable(int variant, int b);
+void launch_sketch_mixed(const SketchPlan& SP, const SlabPlan& P, const float* dMatA,
+                         const float* dMatB, int64_t kc, const int* dScaleExp, int64_t k0,
+                         const double2* dTw, void* dPartial, int accumulate, cudaStream_t s);
+void launch_row_scale_f32(const float* dAT, const float* dB, int64_t n_a, int64_t n_inner,
+                          int64_t n_b, int* dScaleExp, cudaStream_t s);
+void launch_materialize_f32(const SlabPlan& P, const float* dAT, const float* dB, int64_t k0,
+                            int64_t kc, float* dOutA, float* dOutB, cudaStream_t s);
+void launch_f32_to_f64(const float* src, double* dst, int64_t n, cudaStream_t s);
+
 // Top-K over a dense matrix; returns after synchronising s.
 void topk_dense(const double* dC, int64_t n_a, int64_t n_b, int K, uint32_t* dI, uint32_t* dJ,
                 double* dV, cudaStream_t s);

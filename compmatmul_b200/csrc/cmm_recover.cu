@@ -454,4 +454,19 @@ void launch_gemm(int64_t n_a, int64_t n_inner, int64_t n_b, double* dC, const do
   CMM_CUDA(cudaGetLastError());
 }
 
+// ---------------------------------------------------------- conversion
+__global__ void k_f32_to_f64(const float* __restrict__ src, double* __restrict__ dst, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = (double)src[i];
+}
+
+void launch_f32_to_f64(const float* src, double* dst, int64_t n, cudaStream_t s) {
+  if (n <= 0) return;
+  int64_t blocks = (n + 255) / 256;
+  if (blocks > 8 * num_sms()) blocks = 8 * num_sms();
+  count_launch();
+  k_f32_to_f64<<<(unsigned)blocks, 256, 0, s>>>(src, dst, n);
+  CMM_CUDA(cudaGetLastError());
+}
+
 }  // namespace cmm

@@ -526,12 +526,13 @@ __device__ __forceinline__ void seq_addr(const BatchArgs& a, int64_t s, int64_t&
 }
 
 constexpr int kBatchThreads = 256;
+constexpr int kBatchFftCap = 8192;  // complex FP64 per CTA (slabs up to L = 8192)
 
 // inverse complex DFT (sign +1), unnormalised
 __global__ void __launch_bounds__(kBatchThreads) k_batch_ifft(BatchArgs a) {
   extern __shared__ double2 sb[];
   const int M = 1 << a.logM;
-  const int spc = kFftCap >> a.logM;  // sequences per CTA
+  const int spc = kBatchFftCap >> a.logM;  // sequences per CTA
   const int64_t s0 = (int64_t)blockIdx.x * spc;
   const double2* in = reinterpret_cast<const double2*>(a.in);
   for (int e = threadIdx.x; e < (spc << a.logM); e += kBatchThreads) {
@@ -623,10 +624,10 @@ __global__ void __launch_bounds__(kBatchThreads) k_batch_wht(BatchArgs a) {
 }
 
 static void run_batch(bool fft, BatchArgs a, cudaStream_t s) {
-  const int cap = fft ? kFftCap : kWhtCap;
+  const int cap = fft ? kBatchFftCap : kWhtCap;
   const int spc = cap >> a.logM;
   const int64_t blocks = (a.nseq + spc - 1) / spc;
-  const int smem = fft ? kFftCap * (int)sizeof(double2) : kWhtCap * (int)sizeof(double);
+  const int smem = fft ? kBatchFftCap * (int)sizeof(double2) : kWhtCap * (int)sizeof(double);
   count_launch();
   if (fft) {
     CMM_CUDA(cudaFuncSetAttribute(k_batch_ifft, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));

@@ -30,18 +30,31 @@ def _f64_contig(t, name):
         raise ValueError(f"{name} must be a contiguous 2-D float64 CUDA tensor")
 
 
-def compressed_product(AT, B, d, b, seed, variant="fft", hash=None, out=None):
-    """Sketch p (d x b float64 CUDA tensor) of AT^T-layout inputs."""
+def _in_contig(t, name):
+    """float64 (plain path) or float32 (mixed-precision path) inputs."""
     import torch
-    _f64_contig(AT, "AT")
-    _f64_contig(B, "B")
+    if not t.is_cuda or t.dtype not in (torch.float64, torch.float32) or not t.is_contiguous() \
+            or t.dim() != 2:
+        raise ValueError(f"{name} must be a contiguous 2-D float64/float32 CUDA tensor")
+
+
+def compressed_product(AT, B, d, b, seed, variant="fft", hash=None, out=None):
+    """Sketch p (d x b float64 CUDA tensor) of AT^T-layout inputs.  float32
+    inputs take the mixed-precision path."""
+    import torch
+    _in_contig(AT, "AT")
+    _in_contig(B, "B")
+    if AT.dtype != B.dtype:
+        raise ValueError("AT and B must have the same dtype")
     q, n_a = AT.shape
     n_b = B.shape[1]
     if B.shape[0] != q:
         raise ValueError("Shape mismatch! Note that AT is assumed to be transposed")
     p = out if out is not None else torch.empty((d, b), dtype=torch.float64, device=AT.device)
-    check(lib().cmm_dev_compressed_product(VARIANTS[variant], HASH_KINDS[hash], n_a, q, n_b,
-                                           _ptr(AT), _ptr(B), d, b, seed, _ptr(p), _stream(AT)))
+    fn = lib().cmm_dev_compressed_product if AT.dtype == torch.float64 else \
+        lib().cmm_dev_compressed_product_f32
+    check(fn(VARIANTS[variant], HASH_KINDS[hash], n_a, q, n_b, _ptr(AT), _ptr(B), d, b, seed,
+             _ptr(p), _stream(AT)))
     return p
 
 
@@ -54,17 +67,21 @@ def decompress_dense(p, n_a, n_b, d, b, seed, variant="fft", hash=None, out=None
 
 
 def matmul(AT, B, d, b, seed, variant="fft", hash=None, out=None):
-    """Dense estimate C (n_a x n_b) = matmul_{fft,fwht} on the device."""
+    """Dense estimate C (n_a x n_b, float64) = matmul_{fft,fwht} on the
+    device.  float32 inputs take the mixed-precision path."""
     import torch
-    _f64_contig(AT, "AT")
-    _f64_contig(B, "B")
+    _in_contig(AT, "AT")
+    _in_contig(B, "B")
+    if AT.dtype != B.dtype:
+        raise ValueError("AT and B must have the same dtype")
     q, n_a = AT.shape
     n_b = B.shape[1]
     if B.shape[0] != q:
         raise ValueError("Shape mismatch! Note that AT is assumed to be transposed")
     Cm = out if out is not None else torch.empty((n_a, n_b), dtype=torch.float64, device=AT.device)
-    check(lib().cmm_dev_matmul(VARIANTS[variant], HASH_KINDS[hash], n_a, q, n_b, _ptr(Cm), _ptr(AT),
-                               _ptr(B), d, b, seed, _stream(AT)))
+    fn = lib().cmm_dev_matmul if AT.dtype == torch.float64 else lib().cmm_dev_matmul_f32
+    check(fn(VARIANTS[variant], HASH_KINDS[hash], n_a, q, n_b, _ptr(Cm), _ptr(AT), _ptr(B), d, b,
+             seed, _stream(AT)))
     return Cm
 
 

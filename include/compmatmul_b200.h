@@ -133,6 +133,26 @@ int cmm_dev_gemm(int64_t n_a, int64_t n_inner, int64_t n_b, double* dC, const do
                  const double* dB, void* stream);
 
 /* ---------------------------------------------------------------------
+ * Mixed precision (no reference twin: the reference binding accepts FP64
+ * only, compmatmul.cpp:22-30).  FP32 inputs; sketches and transforms in
+ * FP32 with two-sum compensated accumulation over k; FWHT Hadamard-16
+ * factors on the tensor cores (BF16 hi/lo split, FP32 accumulation); the
+ * reduction of the d spectra, the inverse transform, p and C in FP64.
+ * ------------------------------------------------------------------- */
+int cmm_dev_compressed_product_f32(int variant, int hash_kind, int64_t n_a, int64_t n_inner,
+                                   int64_t n_b, const float* dAT, const float* dB, int d, int b,
+                                   uint64_t seed, double* dP, void* stream);
+int cmm_dev_matmul_f32(int variant, int hash_kind, int64_t n_a, int64_t n_inner, int64_t n_b,
+                       double* dC, const float* dAT, const float* dB, int d, int b, uint64_t seed,
+                       void* stream);
+int cmm_compressed_product_f32(int variant, int hash_kind, int64_t n_a, int64_t n_inner,
+                               int64_t n_b, const float* AT, const float* B, int d, int b,
+                               int has_seed, uint64_t seed, double* p_out, uint64_t* seed_out);
+int cmm_matmul_f32(int variant, int hash_kind, int64_t n_a, int64_t n_inner, int64_t n_b,
+                   double* C, const float* AT, const float* B, int d, int b, int has_seed,
+                   uint64_t seed);
+
+/* ---------------------------------------------------------------------
  * Instrumentation for benchmarks (no reference twin).  When enabled, every
  * kernel launch of a family is bracketed by CUDA events recorded on the
  * stream it is launched on.  Families: "hash", "scale", "sketch",

@@ -280,7 +280,7 @@ def _topk_gpu(C_host, K):
     return device.topk(Ct, K)
 
 
-@pytest.mark.parametrize("name", ["config1", "config2_n4096"])
+@pytest.mark.parametrize("name", ["config1", "config2_n4096", "config2_n16384"])
 def test_planted_workload_recovery(gpu, cm, name):
     """Recovered top-K (i, j) set bit-exact vs the reference run on the same
     seeded inputs; values within 1e-10 relative."""
