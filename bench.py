@@ -45,6 +45,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--n", type=int, default=0, help="override the workload size (profiling)")
+    ap.add_argument("--compare-fp64", type=int, default=0,
+                    help="also time N steps of the plain FP64 path on the same inputs")
+    ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"],
+                    help="fp64 = plain path; mixed = FP32 inputs (default for config3)")
     return ap.parse_args()
 
 
@@ -166,7 +170,8 @@ def main():
         w["n"] = args.n
     n, K, d, b = w["n"], w["K"], w["d"], w["b"]
     variant = args.variant
-    config = {"workload": f"{args.workload}: planted-entry A,B {n}x{n} FP64 (noise N(0,0.01^2), "
+    mixed = args.precision == "mixed" or (args.precision == "auto" and w.get("dtype") == "float32")
+    config = {"workload": f"{args.workload}: planted-entry A,B {n}x{n} {'FP32' if mixed else 'FP64'} (noise N(0,0.01^2), "
                           f"K={K} planted +10/+10), {variant.upper()}, b={b}, d={d}, "
                           f"hash=multiply-add-shift; dense median decompression + top-{K}",
               "n": n, "b": b, "d": d, "K": K, "variant": variant,
@@ -210,7 +215,8 @@ def main():
     dv = torch.device("cuda", torch.cuda.current_device())
 
     # inputs: per-rank seeds (independent products), pinned host + HBM copies
-    AT, B, planted = planted_problem(n, n, n, K, w["gen_seed"] + 1000 * rank)
+    AT, B, planted = planted_problem(n, n, n, K, w["gen_seed"] + 1000 * rank,
+                                     dtype=np.float32 if mixed else np.float64)
     hAT = torch.from_numpy(AT).pin_memory()
     hB = torch.from_numpy(B).pin_memory()
     dAT = hAT.to(dv)
@@ -268,8 +274,9 @@ def main():
         if i == 1:
             barrier()
             te0 = time.perf_counter()
-        st = L.cmm_matmul(0 if variant == "fft" else 1, 1, n, n, n, C.c_void_p(hC.data_ptr()),
-                          C.c_void_p(hAT.data_ptr()), C.c_void_p(hB.data_ptr()), d, b, 1, seed)
+        fn = L.cmm_matmul_f32 if mixed else L.cmm_matmul
+        st = fn(0 if variant == "fft" else 1, 1, n, n, n, C.c_void_p(hC.data_ptr()),
+                C.c_void_p(hAT.data_ptr()), C.c_void_p(hB.data_ptr()), d, b, 1, seed)
         cmb.check(st)
     barrier()
     e2e_s = (time.perf_counter() - te0) / e2e_steps
@@ -278,10 +285,26 @@ def main():
         torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
     e2e_value = world / float(te.item())
 
+    # the plain FP64 path on the same (FP32-valued) inputs, for the mixed speed-up
+    fp64_ms = None
+    if mixed and args.compare_fp64:
+        dAT64 = dAT.double()
+        dB64 = dB.double()
+        for i in range(args.compare_fp64 + 1):
+            if i == 1:
+                torch.cuda.synchronize()
+                tf0 = time.perf_counter()
+            dev.matmul(dAT64, dB64, d, b, seed, variant=variant, out=dC)
+            dev.topk(dC, K, as_numpy=False)
+        torch.cuda.synchronize()
+        fp64_ms = (time.perf_counter() - tf0) / args.compare_fp64 * 1e3
+        del dAT64, dB64
+
     # roofline of the dominant kernel (sketch)
     sk_ms, sk_n = fam["sketch"]
     sk_launch_ms = sk_ms / max(1, sk_n)
-    alg_bytes = 8.0 * n * (n + n)  # reads of AT and B per launch
+    esz = 4.0 if mixed else 8.0
+    alg_bytes = esz * n * (n + n)  # reads of AT and B per launch
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (sk_launch_ms / 1e3) / 1e9
     flops = fft_flops(n, n, n, d, b) if variant == "fft" else fwht_ops(n, n, n, d, b)
@@ -292,7 +315,7 @@ def main():
         return
 
     cpu = None
-    if world == 1 and not args.no_cpu_baseline:
+    if world == 1 and not args.no_cpu_baseline and not mixed:
         try:
             sec, thr, sample = cpu_reference_sample(AT, B, n, d, b, variant, seed, args.cpu_seconds)
             cpu = {"value": 1.0 / sec, "unit": "products/s", "cores": thr, "kind": "reference",
@@ -304,7 +327,8 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "products/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (mixed: FP32 transforms, FP64 reduction)" if mixed else "f64",
         "data": "synthetic", "config": config,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": None, "kernel": "k_sketch_fft" if variant == "fft" else "k_sketch_fwht",
@@ -312,13 +336,15 @@ def main():
                      "algorithmic_bytes_per_launch": alg_bytes,
                      "fp64_tflops_achieved": flops / (sk_launch_ms / 1e3) / 1e12},
         "kernel_ms_per_step": {k: v[0] / max(1, args.steps) for k, v in fam.items()},
-        "e2e": {"value": e2e_value, "unit": "products/s", "h2d_bytes_per_step": int(16 * n * n),
+        "e2e": {"value": e2e_value, "unit": "products/s", "h2d_bytes_per_step": int(2 * esz * n * n),
                 "d2h_bytes_per_step": int(8 * n * n)},
         "gpu_launches": int(launches),
         "clocks": clk,
         "recovered_planted": f"{rec}/{K}",
         "cpu_baseline": cpu,
     }
+    if fp64_ms is not None:
+        line["plain_fp64_same_inputs"] = {"ms_per_step": fp64_ms, "speedup": fp64_ms / ms_per_step}
     print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()

@@ -27,8 +27,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                   "--expt-relaxed-constexpr", "-I" + INCLUDE, "-I" + CSRC]
 
-CUDA_SOURCES = ["cmm_sketch.cu", "cmm_sketch_v1.cu", "cmm_sketch_mixed.cu", "cmm_plan.cu",
-                "cmm_recover.cu"]
+CUDA_SOURCES = ["cmm_sketch.cu", "cmm_sketch_v1.cu", "cmm_sketch_mixed.cu", "cmm_sketch_cluster.cu",
+                "cmm_plan.cu", "cmm_recover.cu"]
 HOST_SOURCES = ["cmm_hashparams.cpp", "cmm_capi.cpp"]
 
 

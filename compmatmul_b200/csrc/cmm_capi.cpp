@@ -5,6 +5,7 @@
 //   hash codes -> row balance (FFT) -> fused sketch/transform/accumulate
 //   -> k-group reduction + inverse -> (median decompression) -> (top-K).
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <atomic>
 #include <map>
@@ -176,6 +177,41 @@ static size_t materialize_budget() {
   return free_b / 3 < cap ? free_b / 3 : cap;
 }
 
+// The cluster kernels when this device can co-schedule a cluster of them
+// and the residue segments fit in shared memory; false -> the slab kernels.
+// CMM_SKETCH_KERNELS = cluster | slab forces one family where both apply
+// (for comparisons); unset or "auto" takes the measured-faster choice.
+static int sketch_kernel_choice() {
+  static const int choice = [] {
+    const char* e = getenv("CMM_SKETCH_KERNELS");
+    if (e && !strcmp(e, "cluster")) return 1;
+    if (e && !strcmp(e, "slab")) return 2;
+    return 0;
+  }();
+  return choice;
+}
+
+static bool try_cluster_plan(int variant, bool f32, const Codes& codes, int64_t n_a, int64_t n_b,
+                             int64_t n_inner, const SketchParams& sp, ClusterPlan& C, SlabPlan& plan,
+                             cudaStream_t s) {
+  if (!sketch_cluster_applicable(variant, f32, sp.b)) return false;
+  if (sketch_kernel_choice() == 2) return false;
+  // auto: measured on B200 at n = 16384, d = 9 -- the cluster kernels win for
+  // every FFT case and for FP64 FWHT from R = b / 8192 >= 16 on; FP64 FWHT
+  // at R = 8 ties with the slab kernel, and the tensor-core slab kernel wins
+  // for FP32 FWHT
+  if (sketch_kernel_choice() == 0 && variant == kVariantFWHT && (f32 || sp.b < (1 << 17)))
+    return false;
+  try {
+    C = plan_cluster(variant, f32, n_inner, sp.d, sp.b, 4096);
+  } catch (const unsupported&) {
+    return false;
+  }
+  plan = make_residue_plan(codes.a.as<uint32_t>(), codes.b.as<uint32_t>(), n_a, n_b, sp.d, sp.b,
+                           C.logL, C.logR2, s);
+  return cluster_smem_fits(variant, f32, plan);
+}
+
 static void sketch_device(int variant, const SketchParams& sp, const Codes& codes, int64_t n_a,
                           int64_t n_inner, int64_t n_b, const double* dAT, const double* dB,
                           double* dP, cudaStream_t s) {
@@ -185,6 +221,27 @@ static void sketch_device(int variant, const SketchParams& sp, const Codes& code
   if (variant == kVariantFFT) {
     scale = DevBuf((size_t)(n_inner > 0 ? n_inner : 1) * 4, s);
     launch_row_scale(dAT, dB, n_a, n_inner, n_b, scale.as<int>(), s);
+  }
+  ClusterPlan C;
+  SlabPlan plan;
+  if (n_inner > 0 && try_cluster_plan(variant, false, codes, n_a, n_b, n_inner, sp, C, plan, s)) {
+    // residue plan + per-chunk materialized rows + cluster kernels
+    const int64_t SA = plan.slots_a(), SB = plan.slots_b();
+    const size_t per_row = (size_t)sp.d * (size_t)(SA + SB) * 8;
+    int64_t kc = (int64_t)(materialize_budget() / per_row);
+    if (kc < 1) kc = 1;
+    if (kc > n_inner) kc = n_inner;
+    DevBuf matA((size_t)sp.d * kc * SA * 8, s), matB((size_t)sp.d * kc * SB * 8, s);
+    DevBuf partial((size_t)C.G * sp.d * (size_t)sp.b * elem, s);
+    for (int64_t k0 = 0; k0 < n_inner; k0 += kc) {
+      const int64_t c = n_inner - k0 < kc ? n_inner - k0 : kc;
+      launch_materialize(plan, dAT, dB, k0, c, matA.as<double>(), matB.as<double>(), s);
+      launch_sketch_cluster(variant, false, C, plan, matA.ptr, matB.ptr, c, scale.as<int>(), k0, tw,
+                            partial.ptr, sp.d, k0 > 0 ? 1 : 0, s);
+    }
+    DevBuf work(2 * (size_t)sp.d * (size_t)sp.b * 16, s);
+    launch_finalize_natural(variant, sp.d, sp.b, C.G, partial.ptr, tw, work.ptr, dP, s);
+    return;
   }
   if (n_inner > 0 && sketch_v1_applicable(variant, sp.b, n_a, n_b)) {
     // bucket-sorted plan + per-chunk materialized rows + v1 kernels
@@ -233,6 +290,27 @@ static void sketch_device_mixed(int variant, const SketchParams& sp, const Codes
   const size_t elem = variant == kVariantFFT ? 16 : 8;
   DevBuf scale((size_t)n_inner * 4, s);
   if (variant == kVariantFFT) launch_row_scale_f32(dAT, dB, n_a, n_inner, n_b, scale.as<int>(), s);
+  ClusterPlan Cp;
+  SlabPlan cplan;
+  if (try_cluster_plan(variant, true, codes, n_a, n_b, n_inner, sp, Cp, cplan, s)) {
+    SlabPlan& plan = cplan;
+    const int64_t SA = plan.slots_a(), SB = plan.slots_b();
+    const size_t per_row = (size_t)sp.d * (size_t)(SA + SB) * 4;
+    int64_t kc = (int64_t)(materialize_budget() / per_row);
+    if (kc < 1) kc = 1;
+    if (kc > n_inner) kc = n_inner;
+    DevBuf matA((size_t)sp.d * kc * SA * 4, s), matB((size_t)sp.d * kc * SB * 4, s);
+    DevBuf partial((size_t)Cp.G * sp.d * (size_t)sp.b * elem, s);
+    for (int64_t k0 = 0; k0 < n_inner; k0 += kc) {
+      const int64_t c = n_inner - k0 < kc ? n_inner - k0 : kc;
+      launch_materialize_f32(plan, dAT, dB, k0, c, matA.as<float>(), matB.as<float>(), s);
+      launch_sketch_cluster(variant, true, Cp, plan, matA.ptr, matB.ptr, c, scale.as<int>(), k0, tw,
+                            partial.ptr, sp.d, k0 > 0 ? 1 : 0, s);
+    }
+    DevBuf work(2 * (size_t)sp.d * (size_t)sp.b * 16, s);
+    launch_finalize_natural(variant, sp.d, sp.b, Cp.G, partial.ptr, tw, work.ptr, dP, s);
+    return;
+  }
   const SketchPlan P = plan_sketch_mixed(variant, n_a, n_inner, n_b, sp.d, sp.b, num_sms());
   SlabPlan plan = make_slab_plan(codes.a.as<uint32_t>(), codes.b.as<uint32_t>(), n_a, n_b, sp.d,
                                  sp.b, P.logL, s);

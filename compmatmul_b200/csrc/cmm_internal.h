@@ -141,6 +141,12 @@ constexpr int kPlanThreads = 512;          // threads of the v1 sketch kernels
 constexpr uint32_t kPadSlot = 0xffffffffu;  // slot without an index
 struct SlabPlan {
   int d = 0, logL = 0, EA = 0, EB = 0;
+  int segs = 1;     // residue segments per (t, side): R2 for the cluster kernels
+  bool compact = false;  // residue plans: segments in sorted order, EA/EB = slots per segment,
+                         // countA/countB hold kPlanThreads + 1 cut offsets per segment
+  // slots of one materialized row per t and side
+  int64_t slots_a() const { return (int64_t)segs * EA * (compact ? 1 : kPlanThreads); }
+  int64_t slots_b() const { return (int64_t)segs * EB * (compact ? 1 : kPlanThreads); }
   bool u16 = true;  // codes stored as u16 (b <= 2^16)
   int64_t n_a = 0, n_b = 0;
   DevBuf srcA, srcB;      // d x S: index | (sign == +1) << 31, or kPadSlot
@@ -149,6 +155,9 @@ struct SlabPlan {
 };
 SlabPlan make_slab_plan(const uint32_t* dCodesA, const uint32_t* dCodesB, int64_t n_a, int64_t n_b,
                         int d, int b, int logL, cudaStream_t s);
+// residue plans for the cluster kernels (b = R1 * R2 * L)
+SlabPlan make_residue_plan(const uint32_t* dCodesA, const uint32_t* dCodesB, int64_t n_a, int64_t n_b,
+                           int d, int b, int logL, int logR2, cudaStream_t s);
 void launch_materialize(const SlabPlan& P, const double* dAT, const double* dB, int64_t k0,
                         int64_t kc, double* dOutA, double* dOutB, cudaStream_t s);
 // v1 sketch over materialized rows of inner indices [k0, k0 + kc) (chunk);
@@ -174,6 +183,22 @@ void launch_row_scale_f32(const float* dAT, const float* dB, int64_t n_a, int64_
 void launch_materialize_f32(const SlabPlan& P, const float* dAT, const float* dB, int64_t k0,
                             int64_t kc, float* dOutA, float* dOutB, cudaStream_t s);
 void launch_f32_to_f64(const float* src, double* dst, int64_t n, cudaStream_t s);
+
+// Cluster kernels (cmm_sketch_cluster.cu): b = R1 * R2 * L; partials in
+// natural frequency order [g][t][b].
+struct ClusterPlan {
+  int logL = 0, log2b = 0, logR1 = 0, logR2 = 0, G = 1, max_clusters = 0;
+};
+bool sketch_cluster_applicable(int variant, bool f32, int b);
+ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, int64_t est_slots);
+bool cluster_smem_fits(int variant, bool f32, const SlabPlan& P);
+void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const SlabPlan& P,
+                           const void* dMatA, const void* dMatB, int64_t kc, const int* dScaleExp,
+                           int64_t k0, const double2* dTw, void* dPartial, int d, int accumulate,
+                           cudaStream_t s);
+// finalize for partials in natural frequency order (cluster kernels)
+void launch_finalize_natural(int variant, int d, int b, int G, const void* dPartial,
+                             const double2* dTw, void* dWork, double* dP, cudaStream_t s);
 
 // Top-K over a dense matrix; returns after synchronising s.
 void topk_dense(const double* dC, int64_t n_a, int64_t n_b, int K, uint32_t* dI, uint32_t* dJ,

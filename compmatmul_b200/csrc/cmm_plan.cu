@@ -252,7 +252,7 @@ void launch_materialize(const SlabPlan& P, const double* dAT, const double* dB, 
   if (kc <= 0) return;
   const int64_t nmax = P.n_a > P.n_b ? P.n_a : P.n_b;
   const size_t smem = (size_t)nmax * 8;
-  const int64_t SA = (int64_t)P.EA * kPlanThreads, SB = (int64_t)P.EB * kPlanThreads;
+  const int64_t SA = P.slots_a(), SB = P.slots_b();
   ProfScope prof("materialize", s);
   count_launch();
   if (smem <= 200 * 1024) {
@@ -266,6 +266,199 @@ void launch_materialize(const SlabPlan& P, const double* dAT, const double* dB, 
                                                               SA, SB, kc, dOutA, dOutB);
   }
   CMM_CUDA(cudaGetLastError());
+}
+
+}  // namespace cmm
+
+namespace cmm {
+
+// ------------------------------------------------------ residue plans
+// Plans for the cluster kernels (cmm_sketch_cluster.cu).  With
+// b = R1 * R2 * L, an index with bucket h belongs to residue class
+// r2 = h mod R2 and sub-bucket m = (h mod (b / R1)) div R2 (< L); its DIF
+// quotient is q1 = h div (b / R1).  Per (t, side, r2) the members are
+// stably sorted by m and cut into kPlanThreads ranges at bucket boundaries;
+// slot (s, j) of segment r2 sits at [r2][s * kPlanThreads + j].  The code of
+// a slot is m | q1 << logL.
+constexpr int kSegSortThreads = 1024;
+
+__global__ void __launch_bounds__(kSegSortThreads) k_plan_seg_sort(
+    const uint32_t* __restrict__ codesA, const uint32_t* __restrict__ codesB, int64_t n_a, int64_t n_b,
+    int logL, int logR2, int logM, uint32_t* __restrict__ sortedA, uint32_t* __restrict__ sortedB,
+    uint32_t* __restrict__ cut, uint32_t* __restrict__ emax) {
+  extern __shared__ uint32_t sseg[];
+  const int L = 1 << logL, R2 = 1 << logR2;
+  uint32_t* cnt = sseg;
+  uint32_t* cum = sseg + L + 1;
+  const int t = blockIdx.x, side = blockIdx.y, r2 = blockIdx.z;
+  const int d2 = gridDim.z;
+  const int64_t N = side == 0 ? n_a : n_b;
+  const uint32_t* codes = (side == 0 ? codesA : codesB) + (size_t)t * N;
+  // segment output: sorted[t][r2][0..N) holds the members of residue r2
+  uint32_t* sorted = (side == 0 ? sortedA : sortedB) + ((size_t)t * d2 + r2) * N;
+  const uint32_t rmask = (uint32_t)R2 - 1u, mmask = (1u << logM) - 1u;
+  for (int e = threadIdx.x; e <= L; e += kSegSortThreads) cnt[e] = 0;
+  __syncthreads();
+  for (int64_t i = threadIdx.x; i < N; i += kSegSortThreads) {
+    const uint32_t h = __ldg(codes + i) & 0x7fffffffu;
+    if ((h & rmask) == (uint32_t)r2) atomicAdd(&cnt[(h & mmask) >> logR2], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    const int per = (L + 31) / 32;
+    uint32_t local = 0;
+    for (int e = lane * per; e < (lane + 1) * per && e < L; ++e) local += cnt[e];
+    uint32_t incl = local;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    uint32_t run = incl - local;
+    for (int e = lane * per; e < (lane + 1) * per && e < L; ++e) {
+      const uint32_t c = cnt[e];
+      cum[e] = run;
+      run += c;
+    }
+    if (lane == 31) cum[L] = incl;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e <= L; e += kSegSortThreads) cnt[e] = cum[e];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int64_t base = 0; base < N; base += kSegSortThreads) {
+    const int64_t i = base + threadIdx.x;
+    bool valid = i < N;
+    uint32_t key = 0x80000000u | (uint32_t)lane;
+    if (valid) {
+      const uint32_t h = __ldg(codes + i) & 0x7fffffffu;
+      valid = (h & rmask) == (uint32_t)r2;
+      if (valid) key = (h & mmask) >> logR2;
+    }
+    const uint32_t peers = __match_any_sync(0xffffffffu, key);
+    const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+    for (int w = 0; w < kSegSortThreads / 32; ++w) {
+      if (warp == w && valid) sorted[cnt[key] + rank] = (uint32_t)i;
+      __syncwarp();
+      if (warp == w && valid && rank == 0) cnt[key] += __popc(peers);
+      __syncthreads();
+    }
+  }
+  const uint32_t total = cum[L];
+  uint32_t* cuts = cut + (((size_t)t * 2 + side) * d2 + r2) * (kPlanThreads + 1);
+  for (int j = threadIdx.x; j <= kPlanThreads; j += kSegSortThreads) {
+    const uint64_t target = ((uint64_t)j * (uint64_t)total) / kPlanThreads;
+    int lo = 0, hi = L;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (cum[mid] >= target) hi = mid;
+      else lo = mid + 1;
+    }
+    cuts[j] = j == kPlanThreads ? total : cum[lo];
+  }
+  if (threadIdx.x == 0) emax[((size_t)t * 2 + side) * d2 + r2] = total;  // segment size
+}
+
+template <typename CodeT>
+__global__ void k_plan_seg_layout(const uint32_t* __restrict__ codesA, const uint32_t* __restrict__ codesB,
+                                  int64_t n_a, int64_t n_b, int logL, int logR2, int logM, int R2,
+                                  const uint32_t* __restrict__ sortedA, const uint32_t* __restrict__ sortedB,
+                                  const uint32_t* __restrict__ cut, int SA, int SB,
+                                  uint32_t* __restrict__ srcA, uint32_t* __restrict__ srcB,
+                                  CodeT* __restrict__ codeA, CodeT* __restrict__ codeB,
+                                  uint32_t* __restrict__ cutA, uint32_t* __restrict__ cutB) {
+  const int t = blockIdx.y;
+  const int side = blockIdx.z & 1, r2 = blockIdx.z >> 1;
+  const int S = side == 0 ? SA : SB;
+  const int64_t N = side == 0 ? n_a : n_b;
+  const uint32_t* codes = (side == 0 ? codesA : codesB) + (size_t)t * N;
+  const uint32_t* sorted = (side == 0 ? sortedA : sortedB) + ((size_t)t * R2 + r2) * N;
+  const uint32_t* cuts = cut + (((size_t)t * 2 + side) * R2 + r2) * (kPlanThreads + 1);
+  const uint32_t total = cuts[kPlanThreads];
+  uint32_t* src = (side == 0 ? srcA : srcB) + ((size_t)t * R2 + r2) * S;
+  CodeT* code = (side == 0 ? codeA : codeB) + ((size_t)t * R2 + r2) * S;
+  const uint32_t mmask = (1u << logM) - 1u;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < S; e += (int64_t)gridDim.x * blockDim.x) {
+    if ((uint32_t)e < total) {
+      const uint32_t i = sorted[e];
+      const uint32_t c = codes[i];
+      const uint32_t h = c & 0x7fffffffu;
+      src[e] = i | (c & 0x80000000u);
+      code[e] = (CodeT)(((h & mmask) >> logR2) | ((h >> logM) << logL));
+    } else {
+      src[e] = kPadSlot;
+      code[e] = 0;
+    }
+  }
+  if (blockIdx.x == 0)
+    for (int j = threadIdx.x; j <= kPlanThreads; j += blockDim.x)
+      (side == 0 ? cutA : cutB)[((size_t)t * R2 + r2) * (kPlanThreads + 1) + j] = cuts[j];
+}
+
+SlabPlan make_residue_plan(const uint32_t* dCodesA, const uint32_t* dCodesB, int64_t n_a, int64_t n_b,
+                           int d, int b, int logL, int logR2, cudaStream_t s) {
+  SlabPlan P;
+  P.d = d;
+  P.logL = logL;
+  P.n_a = n_a;
+  P.n_b = n_b;
+  int log2b = 0;
+  while ((1 << log2b) < b) ++log2b;
+  const int logR1 = log2b - logL - logR2;
+  const int logM = log2b - logR1;  // log2(b / R1)
+  P.segs = 1 << logR2;
+  // code = m (logL bits) | q1 << logL (logR1 bits)
+  P.u16 = logL + logR1 <= 16;
+  const int L = 1 << logL, R2 = 1 << logR2;
+  DevBuf sortedA((size_t)d * R2 * (n_a > 0 ? n_a : 1) * 4, s), sortedB((size_t)d * R2 * (n_b > 0 ? n_b : 1) * 4, s);
+  DevBuf cut((size_t)d * 2 * R2 * (kPlanThreads + 1) * 4, s), emax((size_t)d * 2 * R2 * 4, s);
+  const int smem = 2 * (L + 1) * 4;
+  CMM_CUDA(cudaFuncSetAttribute(k_plan_seg_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  {
+    ProfScope prof("plan", s);
+    count_launch();
+    k_plan_seg_sort<<<dim3(d, 2, R2), kSegSortThreads, smem, s>>>(
+        dCodesA, dCodesB, n_a, n_b, logL, logR2, logM, sortedA.as<uint32_t>(), sortedB.as<uint32_t>(),
+        cut.as<uint32_t>(), emax.as<uint32_t>());
+    CMM_CUDA(cudaGetLastError());
+  }
+  std::vector<uint32_t> h((size_t)d * 2 * R2);
+  CMM_CUDA(cudaMemcpyAsync(h.data(), emax.ptr, h.size() * 4, cudaMemcpyDeviceToHost, s));
+  CMM_CUDA(cudaStreamSynchronize(s));
+  // compact segments: S = the largest segment (over t and r2), rounded to 8
+  uint32_t SA = 8, SB = 8;
+  for (int t = 0; t < d; ++t)
+    for (int r = 0; r < R2; ++r) {
+      SA = h[((size_t)t * 2 + 0) * R2 + r] > SA ? h[((size_t)t * 2 + 0) * R2 + r] : SA;
+      SB = h[((size_t)t * 2 + 1) * R2 + r] > SB ? h[((size_t)t * 2 + 1) * R2 + r] : SB;
+    }
+  SA = (SA + 7) & ~7u;
+  SB = (SB + 7) & ~7u;
+  P.compact = true;
+  P.EA = (int)SA;  // slots per segment (not per thread) for compact plans
+  P.EB = (int)SB;
+  const size_t cb = P.u16 ? 2 : 4;
+  P.srcA = DevBuf((size_t)d * R2 * SA * 4, s);
+  P.srcB = DevBuf((size_t)d * R2 * SB * 4, s);
+  P.codeA = DevBuf((size_t)d * R2 * SA * cb, s);
+  P.codeB = DevBuf((size_t)d * R2 * SB * cb, s);
+  P.countA = DevBuf((size_t)d * R2 * (kPlanThreads + 1) * 4, s);
+  P.countB = DevBuf((size_t)d * R2 * (kPlanThreads + 1) * 4, s);
+  const size_t Smax = SA > SB ? SA : SB;
+  dim3 grid((unsigned)((Smax + 255) / 256 < 256 ? (Smax + 255) / 256 : 256), (unsigned)d, (unsigned)(2 * R2));
+  ProfScope prof("plan", s);
+  count_launch();
+#define CMM_SEG_LAYOUT(T)                                                                          \
+  k_plan_seg_layout<T><<<grid, 256, 0, s>>>(dCodesA, dCodesB, n_a, n_b, logL, logR2, logM, R2,      \
+                                            sortedA.as<uint32_t>(), sortedB.as<uint32_t>(),         \
+                                            cut.as<uint32_t>(), (int)SA, (int)SB, P.srcA.as<uint32_t>(), \
+                                            P.srcB.as<uint32_t>(), P.codeA.as<T>(), P.codeB.as<T>(), \
+                                            P.countA.as<uint32_t>(), P.countB.as<uint32_t>())
+  if (P.u16) CMM_SEG_LAYOUT(uint16_t);
+  else CMM_SEG_LAYOUT(uint32_t);
+#undef CMM_SEG_LAYOUT
+  CMM_CUDA(cudaGetLastError());
+  return P;
 }
 
 }  // namespace cmm

@@ -494,6 +494,31 @@ __global__ void k_fft_combine(const double2* partial, int G, int d, int logL, in
   }
 }
 
+// FFT, partials in natural order [g][t][f]: P[f] = (Q[f] - conj(Q[-f]))/(4i),
+// written in the [t][r][m] (f = R m + r) layout the inverse passes read.
+__global__ void k_fft_combine_natural(const double2* partial, int G, int d, int log2b, int logL,
+                                      double2* Pout) {
+  const int64_t b = (int64_t)1 << log2b;
+  const int logR = log2b - logL;
+  const int64_t total = (int64_t)d * b;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int t = (int)(idx >> log2b);
+    const int64_t f = idx & (b - 1);
+    const int64_t fn = (b - f) & (b - 1);
+    double2 Q = make_double2(0.0, 0.0), Qn = make_double2(0.0, 0.0);
+    for (int g = 0; g < G; ++g) {
+      const double2* base = partial + ((size_t)g * d + t) * (size_t)b;
+      const double2 u = base[f], v = base[fn];
+      Q.x += u.x; Q.y += u.y;
+      Qn.x += v.x; Qn.y += v.y;
+    }
+    const double dx = Q.x - Qn.x, dy = Q.y + Qn.y;
+    const int64_t r = f & (((int64_t)1 << logR) - 1), m = f >> logR;
+    Pout[(size_t)t * b + ((size_t)r << logL) + m] = make_double2(0.25 * dy, -0.25 * dx);
+  }
+}
+
 // FWHT: sum of the k-group partials.
 __global__ void k_sum_partials(const double* partial, int G, int64_t n, double* out) {
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n;
@@ -691,6 +716,50 @@ void launch_finalize(const SketchPlan& P, const void* dPartial, const double2* d
     c.tw = dTw; c.log2b = P.log2b; c.post = 0; c.scale = inv_b;
     run_batch(false, c, s);
   }
+}
+
+void launch_finalize_natural(int variant, int d, int b, int G, const void* dPartial,
+                             const double2* dTw, void* dWork, double* dP, cudaStream_t s) {
+  SketchPlan P{};
+  P.variant = variant;
+  P.d = d;
+  P.b = b;
+  P.log2b = 0;
+  while ((1 << P.log2b) < b) ++P.log2b;
+  P.logL = P.log2b < 12 ? P.log2b : 12;
+  P.L = 1 << P.logL;
+  P.logR = P.log2b - P.logL;
+  P.R = 1 << P.logR;
+  P.G = G;
+  if (variant != kVariantFFT) {
+    // FWHT partials are already in natural order = the [t][r][m] layout
+    launch_finalize(P, dPartial, dTw, dWork, dP, s);
+    return;
+  }
+  const int64_t db = (int64_t)d * b;
+  int64_t blocks = (db + 255) / 256;
+  if (blocks > 8192) blocks = 8192;
+  ProfScope prof("finalize", s);
+  count_launch(3);
+  double2* w1 = reinterpret_cast<double2*>(dWork);
+  double2* w2 = w1 + db;
+  k_fft_combine_natural<<<(unsigned)blocks, 256, 0, s>>>(reinterpret_cast<const double2*>(dPartial), G, d,
+                                                         P.log2b, P.logL, w1);
+  CMM_CUDA(cudaGetLastError());
+  BatchArgs a{};
+  a.in = w1; a.out = w2; a.logM = P.logL;
+  a.nseq = (int64_t)P.d * P.R; a.inner = P.R;
+  a.is1 = P.b; a.is2 = P.L; a.ie = 1;
+  a.os1 = P.b; a.os2 = P.L; a.oe = 1;
+  a.tw = dTw; a.log2b = P.log2b; a.post = 1; a.scale = 1.0;
+  run_batch(true, a, s);
+  BatchArgs c{};
+  c.in = w2; c.out = dP; c.logM = P.logR;
+  c.nseq = (int64_t)P.d * P.L; c.inner = P.L;
+  c.is1 = P.b; c.is2 = 1; c.ie = P.L;
+  c.os1 = P.b; c.os2 = 1; c.oe = P.L;
+  c.tw = dTw; c.log2b = P.log2b; c.post = 2; c.scale = 1.0 / (double)P.b;
+  run_batch(true, c, s);
 }
 
 }  // namespace cmm

@@ -1,0 +1,798 @@
+// Cluster sketch kernels: the hot path for large b.
+//
+// With b = R1 * R2 * L:
+//  * a radix-R1 decimation in frequency splits the b frequencies into R1
+//    interleaved slabs (f = R1 f' + r1 for the FFT; f = r1 (b / R1) + f' for
+//    the FWHT); each slab is a length M = b / R1 transform of
+//      u_r1[n1] = tw(n1, r1) * sum_q1 w(q1, r1) x[q1 M + n1];
+//  * a thread-block cluster of R2 CTAs computes one slab by decimation in
+//    time: CTA r2 takes the members of residue class n1 mod R2 only (the
+//    bucket-sorted plan hands each CTA its own segment of every row, so an
+//    index is scattered by R1 CTAs instead of by every slab), sums them into
+//    its length-L sub-sequence and transforms it in shared memory;
+//  * the R2 sub-spectra are combined by a radix-R2 DFT/WHT across the
+//    cluster, reading the other CTAs' shared memory (DSMEM): CTA r2 owns the
+//    frequencies of L / R2 sub-spectrum positions and accumulates
+//    Z^2 (FFT, z = alpha x + i beta y) or X * Y (FWHT) for them over k.
+//  Two cluster barriers per inner index keep the sub-spectra alive while
+//  they are read.  Every CTA of a cluster runs the same k loop, so all of
+//  them reach every barrier.
+// Instantiations: FFT/FWHT x FP64/FP32 (FP32 = mixed precision: FP32 data,
+// two-sum compensated accumulation, tensor-core Hadamard-16 stages for the
+// FWHT, FP64 partials).
+#include <cooperative_groups.h>
+#include <cuda_bf16.h>
+
+#include <cstdio>
+#include <cstdlib>
+
+#include "cmm_internal.h"
+
+namespace cg = cooperative_groups;
+
+namespace cmm {
+namespace {
+
+constexpr int kCT = kPlanThreads;  // 512
+constexpr int kCBatch = 8;
+constexpr int kCSkip = -0x7fffffff;
+
+// -------------------------------------------------------- complex helpers
+__device__ __forceinline__ double2 mk(double x, double y) { return make_double2(x, y); }
+__device__ __forceinline__ float2 mk(float x, float y) { return make_float2(x, y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return mk(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return mk(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+template <typename C>
+__device__ __forceinline__ void bf(C& a, C& b, C w) {
+  const C t = cmul(b, w);
+  b = mk(a.x - t.x, a.y - t.y);
+  a = mk(a.x + t.x, a.y + t.y);
+}
+template <typename C>
+__device__ __forceinline__ C csq(C a) {
+  return mk(a.x * a.x - a.y * a.y, (a.x + a.x) * a.y);
+}
+
+// three radix-2 DIT stages on x[0..7] (points base + e*half); W = w_{8half}^kk
+template <typename C>
+__device__ __forceinline__ void r8(C (&x)[8], C W) {
+  using R = decltype(W.x);
+  const R h = (R)0.70710678118654752440;
+  const C W2 = csq(W), W4 = csq(W2);
+  bf(x[0], x[1], W4); bf(x[2], x[3], W4); bf(x[4], x[5], W4); bf(x[6], x[7], W4);
+  const C W2m = mk(W2.y, -W2.x);
+  bf(x[0], x[2], W2); bf(x[4], x[6], W2); bf(x[1], x[3], W2m); bf(x[5], x[7], W2m);
+  const C W1 = cmul(W, mk(h, -h));
+  const C Wi = mk(W.y, -W.x);
+  const C W3 = cmul(W, mk(-h, -h));
+  bf(x[0], x[4], W); bf(x[1], x[5], W1); bf(x[2], x[6], Wi); bf(x[3], x[7], W3);
+}
+
+// DFT_8 with natural-order input and output
+template <typename C>
+__device__ __forceinline__ void dft8(C (&u)[8]) {
+  C x[8] = {u[0], u[4], u[2], u[6], u[1], u[5], u[3], u[7]};
+  using R = decltype(u[0].x);
+  r8(x, mk((R)1, (R)0));
+#pragma unroll
+  for (int e = 0; e < 8; ++e) u[e] = x[e];
+}
+
+template <typename R, int M>
+__device__ __forceinline__ void whtr(R (&x)[M]) {
+#pragma unroll
+  for (int h = 1; h < M; h <<= 1)
+#pragma unroll
+    for (int e = 0; e < M; ++e)
+      if (!(e & h)) {
+        const R a = x[e], b = x[e + h];
+        x[e] = a + b;
+        x[e + h] = a - b;
+      }
+}
+
+__device__ __forceinline__ void tsum(float& hi, float& lo, float x) {
+  const float s = hi + x;
+  const float bp = s - hi;
+  lo += (hi - (s - bp)) + (x - bp);
+  hi = s;
+}
+
+// padded shared layouts: 16-byte elements p + p/8, 8-byte p + p/16, 4-byte p + p/32
+template <int ES>
+__device__ __forceinline__ int phys(int p) {
+  return ES == 16 ? p + (p >> 3) : (ES == 8 ? p + (p >> 4) : p + (p >> 5));
+}
+template <int ES>
+constexpr int phys_len(int L) {
+  return ES == 16 ? L + L / 8 : (ES == 8 ? L + L / 16 : L + L / 32);
+}
+
+// ------------------------------------------------- tensor-core H16 (FP32)
+__device__ __forceinline__ uint32_t bf16x2(float lo_e, float hi_e) {
+  return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(lo_e)) |
+         ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(hi_e)) << 16);
+}
+__device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_t& lo) {
+  const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
+  hi = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+  lo = bf16x2(x0 - __bfloat162float(h0), x1 - __bfloat162float(h1));
+}
+__device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+template <int STAGE>
+__device__ __forceinline__ int hpt(int V, int e) {
+  if (STAGE == 0) return V * 16 + e;
+  if (STAGE == 1) return (V >> 4) * 256 + e * 16 + (V & 15);
+  return (V >> 8) * 4096 + e * 256 + (V & 255);
+}
+template <int STAGE>
+__device__ __forceinline__ void h16(float* buf, const uint32_t (&hb)[2][2], int warp, int lane) {
+  const int gq = lane >> 2, tq = lane & 3;
+  for (int tile = warp; tile < 32; tile += kCT / 32) {
+    const int V0 = tile * 16;
+    const int p[8] = {hpt<STAGE>(V0 + gq, 2 * tq),     hpt<STAGE>(V0 + gq, 2 * tq + 1),
+                      hpt<STAGE>(V0 + gq + 8, 2 * tq), hpt<STAGE>(V0 + gq + 8, 2 * tq + 1),
+                      hpt<STAGE>(V0 + gq, 2 * tq + 8), hpt<STAGE>(V0 + gq, 2 * tq + 9),
+                      hpt<STAGE>(V0 + gq + 8, 2 * tq + 8), hpt<STAGE>(V0 + gq + 8, 2 * tq + 9)};
+    float x[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) x[e] = buf[phys<4>(p[e])];
+    uint32_t ahi[4], alo[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) split2(x[2 * e], x[2 * e + 1], ahi[e], alo[e]);
+    float c0[4] = {0.f, 0.f, 0.f, 0.f}, c1[4] = {0.f, 0.f, 0.f, 0.f};
+    mma16816(c0, ahi, hb[0][0], hb[0][1]);
+    mma16816(c0, alo, hb[0][0], hb[0][1]);
+    mma16816(c1, ahi, hb[1][0], hb[1][1]);
+    mma16816(c1, alo, hb[1][0], hb[1][1]);
+    const float y[8] = {c0[0], c0[1], c0[2], c0[3], c1[0], c1[1], c1[2], c1[3]};
+#pragma unroll
+    for (int e = 0; e < 8; ++e) buf[phys<4>(p[e])] = y[e];
+  }
+}
+
+}  // namespace
+
+struct ClArgs {
+  const void* matA;  // [t][kk][R2][SA]
+  const void* matB;
+  const void* codeA;  // [t][R2][SA]
+  const void* codeB;
+  const uint32_t* countA;  // [t][R2][512]
+  const uint32_t* countB;
+  const int* scale_exp;
+  const double2* tw;  // w_b^j
+  void* partial;      // [g][t][b] double2 (FFT) / double (FWHT)
+  int64_t SA, SB, kc, k0;
+  int d, log2b, logR1, logR2, G, accumulate;
+};
+
+// VARIANT 0 = FFT, 1 = FWHT; Real = double (plain) or float (mixed)
+template <int VARIANT, typename Real, typename CodeT>
+__global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
+  constexpr bool kFFT = VARIANT == kVariantFFT;
+  constexpr bool kF32 = sizeof(Real) == 4;
+  constexpr int LOGL = (kFFT && !kF32) ? 12 : 13;
+  constexpr int L = 1 << LOGL;
+  using C = typename std::conditional<kF32, float2, double2>::type;
+  constexpr int ES = kFFT ? (int)sizeof(C) : (int)sizeof(Real);  // shared element size
+  constexpr int PL = phys_len<ES>(L);
+  constexpr int OUT = L / kCT;  // outputs per thread (8 or 16)
+
+  extern __shared__ __align__(16) unsigned char sm[];
+  cg::cluster_group cluster = cg::this_cluster();
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int R1 = 1 << a.logR1, R2 = 1 << a.logR2;
+  const int r2 = (int)cluster.block_rank();
+  const int logM = a.log2b - a.logR1;  // M = b / R1
+  const double2* tw = a.tw;
+
+  // ---- shared layout
+  unsigned char* p = sm;
+  C* buf = nullptr;     // FFT: L complex
+  Real* xs = nullptr;   // FWHT: L real (A side)
+  Real* ys = nullptr;   // FWHT: L real (B side)
+  if (kFFT) { buf = reinterpret_cast<C*>(p); p += PL * sizeof(C); }
+  else { xs = reinterpret_cast<Real*>(p); ys = xs + PL; p += 2 * PL * sizeof(Real); }
+  C* post = reinterpret_cast<C*>(p);            // FFT: w_M^{n r2}, n < L
+  if (kFFT) p += L * sizeof(C);
+  C* preHi = reinterpret_cast<C*>(p);           // FFT, R1 > 1: w_b^{x}, x = hi * 512 + lo
+  C* preLo = preHi + 1024;
+  if (kFFT) p += (1024 + 512) * sizeof(C);
+  C* ptw = reinterpret_cast<C*>(p);             // FFT pass twiddles (<= 1176)
+  if (kFFT) p += 1184 * sizeof(C);
+  Real* wRx = reinterpret_cast<Real*>(p);       // FFT: Re/Im w_R1^j, j < 16
+  Real* wRy = wRx + 16;
+  p += 32 * sizeof(Real);
+  CodeT* cA = reinterpret_cast<CodeT*>(p);
+  CodeT* cB = cA + a.SA;
+
+  // ---- tables (constant over k)
+  if (kFFT) {
+    for (int n = tid; n < L; n += kCT) {
+      const double2 w = tw[((uint64_t)n * (uint64_t)r2) << a.logR1];  // w_M^{n r2} = w_b^{n r2 R1}
+      post[n] = mk((Real)w.x, (Real)w.y);
+    }
+    if (R1 > 1) {
+      for (int e = tid; e < 1024; e += kCT) {
+        const uint64_t x = (uint64_t)e << 9;
+        const double2 w = x < ((uint64_t)1 << a.log2b) ? tw[x] : make_double2(1.0, 0.0);
+        preHi[e] = mk((Real)w.x, (Real)w.y);
+      }
+      for (int e = tid; e < 512; e += kCT) {
+        const double2 w = tw[e];
+        preLo[e] = mk((Real)w.x, (Real)w.y);
+      }
+    }
+    // pass twiddles w_{8 half}^kk at half = 8^p (FP64: 3 passes after the
+    // first) or 16 * 8^(p-1) (FP32), and w_16^k for the cluster combine
+    if (!kF32) {
+      // [0,8) w_64, [8,72) w_512, [72,584) w_4096, [584,592) w_16
+      for (int e = tid; e < 8 + 64 + 512 + 8; e += kCT) {
+        const int lg = e < 8 ? 6 : (e < 72 ? 9 : (e < 584 ? 12 : 4));
+        const int kk = e < 8 ? e : (e < 72 ? e - 8 : (e < 584 ? e - 72 : e - 584));
+        const double2 w = tw[(uint32_t)kk << (a.log2b - lg)];
+        ptw[e] = mk((Real)w.x, (Real)w.y);
+      }
+    } else {
+      for (int e = tid; e < 16 + 128 + 1024 + 8; e += kCT) {
+        int lg, kk;
+        if (e < 16) { lg = 7; kk = e; }
+        else if (e < 144) { lg = 10; kk = e - 16; }
+        else if (e < 1168) { lg = 13; kk = e - 144; }
+        else { lg = 4; kk = e - 1168; }
+        const double2 w = tw[(uint32_t)kk << (a.log2b - lg)];
+        ptw[e] = mk((Real)w.x, (Real)w.y);
+      }
+    }
+    for (int e = tid; e < 16; e += kCT) {
+      const double2 w = e < R1 ? tw[(uint32_t)e << logM] : make_double2(1.0, 0.0);  // w_R1^e
+      wRx[e] = (Real)w.x;
+      wRy[e] = (Real)w.y;
+    }
+  }
+  // B fragments of H16 for the FP32 FWHT
+  uint32_t hb[2][2] = {{0u, 0u}, {0u, 0u}};
+  if (!kFFT && kF32) {
+    const int gq = lane >> 2, tq = lane & 3;
+#pragma unroll
+    for (int hf = 0; hf < 2; ++hf) {
+      const int c = gq + 8 * hf;
+      auto hv = [](int e, int cc) { return (__popc(e & cc) & 1) ? -1.f : 1.f; };
+      hb[hf][0] = bf16x2(hv(2 * tq, c), hv(2 * tq + 1, c));
+      hb[hf][1] = bf16x2(hv(2 * tq + 8, c), hv(2 * tq + 9, c));
+    }
+  }
+
+  // ---- persistent loop over work items (r1, t, k-group); every CTA of a
+  // cluster has the same blockIdx.y, hence the same items and barriers
+  const int items = (R1 * a.d) * a.G;
+  for (int item = blockIdx.y; item < items; item += gridDim.y) {
+  const int r1 = item & (R1 - 1);
+  const int t = (item >> a.logR1) % a.d;
+  const int g = (item >> a.logR1) / a.d;
+  __syncthreads();  // the previous item is done with the shared codes
+  // codes of this CTA's segment, premixed with the DIF weight index for r1
+  {
+    const CodeT* gA = reinterpret_cast<const CodeT*>(a.codeA) + ((size_t)t * R2 + r2) * a.SA;
+    const CodeT* gB = reinterpret_cast<const CodeT*>(a.codeB) + ((size_t)t * R2 + r2) * a.SB;
+    for (int64_t e = tid; e < a.SA + a.SB; e += kCT) {
+      const uint32_t h = e < a.SA ? (uint32_t)gA[e] : (uint32_t)gB[e - a.SA];
+      const uint32_t m = h & (L - 1), q1 = h >> LOGL;
+      const uint32_t w = kFFT ? ((q1 * (uint32_t)r1) & (uint32_t)(R1 - 1)) : (__popc(q1 & (uint32_t)r1) & 1u);
+      (e < a.SA ? cA[e] : cB[e - a.SA]) = (CodeT)(m | (w << LOGL));
+    }
+  }
+  // this thread's contiguous slot range in its segment (compact plan)
+  const uint32_t* cutA = a.countA + ((size_t)t * R2 + r2) * (kCT + 1);
+  const uint32_t* cutB = a.countB + ((size_t)t * R2 + r2) * (kCT + 1);
+  const int begA = (int)cutA[tid], endA = (int)cutA[tid + 1];
+  const int begB = (int)cutB[tid], endB = (int)cutB[tid + 1];
+
+  // ---- accumulators for this CTA's outputs
+  // group gi = tid + 512 u (u < OUT / 8) covers sub-spectrum position
+  // n = r2 * (L / R2) + (gi >> (logR2 - 3)) and 8 of its R2 outputs
+  const int64_t bsz = (int64_t)1 << a.log2b;
+  auto out_f = [&](int gi, int jj) -> int64_t {
+    const int nl = gi >> (a.logR2 - 3);
+    const int half = gi & ((R2 >> 3) - 1);
+    const int n = r2 * (L >> a.logR2) + nl;
+    if (kFFT) {
+      const int j = R2 == 16 ? 2 * jj + half : jj;
+      return ((int64_t)n + (int64_t)L * j) * R1 + r1;
+    } else {
+      const int j = R2 == 16 ? half * 8 + jj : jj;
+      return (int64_t)r1 * (bsz >> a.logR1) + (int64_t)n * R2 + j;
+    }
+  };
+  double2* partC = reinterpret_cast<double2*>(a.partial) + ((size_t)g * a.d + t) * (size_t)bsz;
+  double* partR = reinterpret_cast<double*>(a.partial) + ((size_t)g * a.d + t) * (size_t)bsz;
+  constexpr int QC = kFFT ? 2 : 1;  // components per accumulator
+  double qd[OUT][QC];  // FP64 accumulators (FP64 path)
+  float qh[OUT][QC], ql[OUT][QC];  // two-sum pairs (FP32 path)
+#pragma unroll
+  for (int o = 0; o < OUT; ++o) {
+    const int gi = tid + kCT * (o >> 3);
+    const int64_t f = out_f(gi, o & 7);
+    double vx = 0.0, vy = 0.0;
+    if (a.accumulate) {
+      if (kFFT) { const double2 v = partC[f]; vx = v.x; vy = v.y; }
+      else vx = partR[f];
+    }
+    if (kF32) {
+      qh[o][0] = (float)vx; ql[o][0] = (float)(vx - (double)qh[o][0]);
+      if (kFFT) { qh[o][QC - 1] = (float)vy; ql[o][QC - 1] = (float)(vy - (double)qh[o][QC - 1]); }
+    } else {
+      qd[o][0] = vx;
+      if (kFFT) qd[o][QC - 1] = vy;
+    }
+  }
+
+  const int64_t per = (a.kc + a.G - 1) / a.G;
+  const int64_t kb = (int64_t)g * per;
+  const int64_t ke = kb + per < a.kc ? kb + per : a.kc;
+  cluster.sync();
+
+  for (int64_t kk = kb; kk < ke; ++kk) {
+    Real alpha = (Real)1, beta = (Real)1;
+    if (kFFT) {
+      const int se = __ldg(a.scale_exp + a.k0 + kk);
+      if (se == kCSkip) continue;  // the same for every CTA of the cluster
+      alpha = kF32 ? (Real)__int_as_float((127 - se) << 23) : (Real)__longlong_as_double((long long)(1023 - se) << 52);
+      beta = kF32 ? (Real)__int_as_float((127 + se) << 23) : (Real)__longlong_as_double((long long)(1023 + se) << 52);
+      for (int e = tid; e < PL; e += kCT) buf[e] = mk((Real)0, (Real)0);
+    } else {
+      for (int e = tid; e < PL; e += kCT) { xs[e] = (Real)0; ys[e] = (Real)0; }
+    }
+    __syncthreads();
+    // ---- scatter this CTA's residue segment (run accumulation, one store per bucket)
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      const Real* row = reinterpret_cast<const Real*>(side == 0 ? a.matA : a.matB) +
+                        (((size_t)t * a.kc + kk) * R2 + r2) * (side == 0 ? a.SA : a.SB);
+      const CodeT* codes = side == 0 ? cA : cB;
+      const int beg = side == 0 ? begA : begB, end = side == 0 ? endA : endB;
+      const Real sc = side == 0 ? alpha : beta;
+      uint32_t cur = 0xffffffffu;
+      C acc = mk((Real)0, (Real)0);
+      auto flush = [&](uint32_t m) {
+        if (kFFT) {
+          const uint32_t pos = __brev(m) >> (32 - LOGL);
+          C& dst = buf[phys<ES>((int)pos)];
+          if (side == 0) dst = mk(acc.x * sc, acc.y * sc);
+          else dst = mk(fma(acc.x, sc, dst.x), fma(acc.y, sc, dst.y));
+        } else {
+          (side == 0 ? xs : ys)[phys<ES>((int)m)] = acc.x;
+        }
+      };
+      for (int s0 = beg; s0 < end; s0 += kCBatch) {
+        Real vv[kCBatch];
+        uint32_t hh[kCBatch];
+#pragma unroll
+        for (int u = 0; u < kCBatch; ++u) {
+          const bool ok = s0 + u < end;
+          const int e = s0 + u;
+          vv[u] = ok ? __ldg(row + e) : (Real)0;
+          hh[u] = ok ? (uint32_t)codes[e] : 0xffffffffu;
+        }
+#pragma unroll
+        for (int u = 0; u < kCBatch; ++u) {
+          if (hh[u] == 0xffffffffu) break;
+          const uint32_t h = hh[u];
+          const uint32_t m = h & (L - 1), w = h >> LOGL;
+          C c;
+          if (kFFT) {
+            const Real wx = wRx[w], wy = wRy[w];
+            c = side == 0 ? mk(vv[u] * wx, vv[u] * wy) : mk(-vv[u] * wy, vv[u] * wx);
+          } else {
+            c = mk(w ? -vv[u] : vv[u], (Real)0);
+          }
+          if (m != cur) {
+            if (cur != 0xffffffffu) flush(cur);
+            cur = m;
+            acc = c;
+          } else {
+            acc.x += c.x;
+            acc.y += c.y;
+          }
+        }
+      }
+      if (cur != 0xffffffffu) flush(cur);
+      if (kFFT) __syncthreads();
+    }
+    if (!kFFT) __syncthreads();
+
+    // ---- local transform of length L (results stay in shared memory)
+    if (kFFT && !kF32) {
+      // 4 radix-8 DIT passes; pass 0 applies the DIF twiddle w_b^{n1 r1}
+#pragma unroll
+      for (int ps = 0; ps < 4; ++ps) {
+        const int s0 = 3 * ps, half = 1 << s0;
+        const int kk2 = tid & (half - 1);
+        const int base = ((tid >> s0) << (s0 + 3)) | kk2;
+        C x[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) x[e] = buf[phys<ES>(base + e * half)];
+        if (ps == 0 && R1 > 1) {
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            const uint32_t m = __brev((uint32_t)(base + e)) >> (32 - LOGL);
+            const uint32_t xx = ((m << a.logR2) + (uint32_t)r2) * (uint32_t)r1;  // n1 r1 < b
+            x[e] = cmul(x[e], cmul(preHi[xx >> 9], preLo[xx & 511]));
+          }
+        }
+        r8(x, ps == 0 ? mk((Real)1, (Real)0) : ptw[(ps == 1 ? 0 : (ps == 2 ? 8 : 72)) + kk2]);
+        if (ps == 3) {
+#pragma unroll
+          for (int e = 0; e < 8; ++e) x[e] = cmul(x[e], post[base + e * half]);
+        }
+#pragma unroll
+        for (int e = 0; e < 8; ++e) buf[phys<ES>(base + e * half)] = x[e];
+        __syncthreads();
+      }
+    } else if (kFFT) {
+      // FP32, L = 8192: radix-16 (stages 0-3) + 3 radix-8 passes
+      {
+        const int base = tid * 16;
+        C x[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) x[e] = buf[phys<ES>(base + e)];
+        if (R1 > 1) {
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            const uint32_t m = __brev((uint32_t)(base + e)) >> (32 - LOGL);
+            const uint32_t xx = ((m << a.logR2) + (uint32_t)r2) * (uint32_t)r1;
+            x[e] = cmul(x[e], cmul(preHi[xx >> 9], preLo[xx & 511]));
+          }
+        }
+#pragma unroll
+        for (int st = 0; st < 4; ++st) {
+          const int hh = 1 << st;
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            if (e & hh) continue;
+            bf(x[e], x[e + hh], ptw[1168 + (e & (hh - 1)) * (8 >> st)]);
+          }
+        }
+#pragma unroll
+        for (int e = 0; e < 16; ++e) buf[phys<ES>(base + e)] = x[e];
+      }
+      __syncthreads();
+#pragma unroll
+      for (int ps = 1; ps <= 3; ++ps) {
+        const int s0 = ps == 1 ? 4 : (ps == 2 ? 7 : 10), half = 1 << s0;
+#pragma unroll
+        for (int gg = 0; gg < 2; ++gg) {
+          const int gi = tid + gg * kCT;
+          const int kk2 = gi & (half - 1);
+          const int base = ((gi >> s0) << (s0 + 3)) | kk2;
+          C x[8];
+#pragma unroll
+          for (int e = 0; e < 8; ++e) x[e] = buf[phys<ES>(base + e * half)];
+          r8(x, ptw[(ps == 1 ? 0 : (ps == 2 ? 16 : 144)) + kk2]);
+          if (ps == 3) {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) x[e] = cmul(x[e], post[base + e * half]);
+          }
+#pragma unroll
+          for (int e = 0; e < 8; ++e) buf[phys<ES>(base + e * half)] = x[e];
+        }
+        __syncthreads();
+      }
+    } else if (!kF32) {
+      // FP64 WHT of x and y: radix-16 + 3 radix-8 passes, natural order
+      {
+        const int base = tid * 16;
+        Real x[16], y[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) { x[e] = xs[phys<ES>(base + e)]; y[e] = ys[phys<ES>(base + e)]; }
+        whtr<Real, 16>(x);
+        whtr<Real, 16>(y);
+#pragma unroll
+        for (int e = 0; e < 16; ++e) { xs[phys<ES>(base + e)] = x[e]; ys[phys<ES>(base + e)] = y[e]; }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int ps = 1; ps <= 3; ++ps) {
+        const int s0 = ps == 1 ? 4 : (ps == 2 ? 7 : 10), half = 1 << s0;
+#pragma unroll
+        for (int gg = 0; gg < 2; ++gg) {
+          const int gi = tid + gg * kCT;
+          const int base = ((gi >> s0) << (s0 + 3)) | (gi & (half - 1));
+          Real x[8], y[8];
+#pragma unroll
+          for (int e = 0; e < 8; ++e) { x[e] = xs[phys<ES>(base + e * half)]; y[e] = ys[phys<ES>(base + e * half)]; }
+          whtr<Real, 8>(x);
+          whtr<Real, 8>(y);
+#pragma unroll
+          for (int e = 0; e < 8; ++e) { xs[phys<ES>(base + e * half)] = x[e]; ys[phys<ES>(base + e * half)] = y[e]; }
+        }
+        __syncthreads();
+      }
+    } else {
+      // FP32 WHT: three Hadamard-16 factors on the tensor cores + radix-2
+      float* fx = reinterpret_cast<float*>(xs);
+      float* fy = reinterpret_cast<float*>(ys);
+      h16<0>(fx, hb, warp, lane);
+      h16<0>(fy, hb, warp, lane);
+      __syncthreads();
+      h16<1>(fx, hb, warp, lane);
+      h16<1>(fy, hb, warp, lane);
+      __syncthreads();
+      h16<2>(fx, hb, warp, lane);
+      h16<2>(fy, hb, warp, lane);
+      __syncthreads();
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const int m = tid + kCT * e;
+        const float x0 = fx[phys<ES>(m)], x1 = fx[phys<ES>(m + 4096)];
+        const float y0 = fy[phys<ES>(m)], y1 = fy[phys<ES>(m + 4096)];
+        fx[phys<ES>(m)] = x0 + x1; fx[phys<ES>(m + 4096)] = x0 - x1;
+        fy[phys<ES>(m)] = y0 + y1; fy[phys<ES>(m + 4096)] = y0 - y1;
+      }
+      __syncthreads();
+    }
+
+    cluster.sync();  // every sub-spectrum of the cluster is complete
+
+    // ---- radix-R2 combine across the cluster; accumulate
+#pragma unroll
+    for (int u = 0; u < OUT / 8; ++u) {
+      const int gi = tid + kCT * u;
+      const int nl = gi >> (a.logR2 - 3);
+      const int half = gi & ((R2 >> 3) - 1);
+      const int n = r2 * (L >> a.logR2) + nl;
+      if (kFFT) {
+        C z[8];
+        if (R2 == 16) {
+#pragma unroll
+          for (int r = 0; r < 8; ++r) {
+            const C* b0 = cluster.map_shared_rank(buf, r);
+            const C* b8 = cluster.map_shared_rank(buf, r + 8);
+            const C lo = b0[phys<ES>(n)], hi = b8[phys<ES>(n)];
+            // even outputs: z_r + z_{r+8}; odd outputs: w_16^r (z_r - z_{r+8})
+            if (half == 0) z[r] = mk(lo.x + hi.x, lo.y + hi.y);
+            else z[r] = cmul(mk(lo.x - hi.x, lo.y - hi.y), ptw[(kF32 ? 1168 : 584) + r]);
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < 8; ++r) z[r] = cluster.map_shared_rank(buf, r)[phys<ES>(n)];
+        }
+        dft8(z);
+#pragma unroll
+        for (int jj = 0; jj < 8; ++jj) {
+          const int o = u * 8 + jj;
+          const Real zr = z[jj].x * z[jj].x - z[jj].y * z[jj].y;
+          const Real zi = (z[jj].x + z[jj].x) * z[jj].y;
+          if (kF32) {
+            tsum(qh[o][0], ql[o][0], (float)zr);
+            tsum(qh[o][QC - 1], ql[o][QC - 1], (float)zi);
+          } else {
+            qd[o][0] += (double)zr;
+            qd[o][QC - 1] += (double)zi;
+          }
+        }
+      } else {
+        Real zx[8], zy[8];
+        if (R2 == 16) {
+#pragma unroll
+          for (int r = 0; r < 8; ++r) {
+            const Real* x0 = cluster.map_shared_rank(xs, r);
+            const Real* x8 = cluster.map_shared_rank(xs, r + 8);
+            const Real* y0 = cluster.map_shared_rank(ys, r);
+            const Real* y8 = cluster.map_shared_rank(ys, r + 8);
+            const Real a0 = x0[phys<ES>(n)], a8 = x8[phys<ES>(n)];
+            const Real c0 = y0[phys<ES>(n)], c8 = y8[phys<ES>(n)];
+            zx[r] = half == 0 ? a0 + a8 : a0 - a8;
+            zy[r] = half == 0 ? c0 + c8 : c0 - c8;
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < 8; ++r) {
+            zx[r] = cluster.map_shared_rank(xs, r)[phys<ES>(n)];
+            zy[r] = cluster.map_shared_rank(ys, r)[phys<ES>(n)];
+          }
+        }
+        whtr<Real, 8>(zx);
+        whtr<Real, 8>(zy);
+#pragma unroll
+        for (int jj = 0; jj < 8; ++jj) {
+          const int o = u * 8 + jj;
+          if (kF32) tsum(qh[o][0], ql[o][0], (float)(zx[jj] * zy[jj]));
+          else qd[o][0] = fma((double)zx[jj], (double)zy[jj], qd[o][0]);
+        }
+      }
+    }
+    cluster.sync();  // all reads of the sub-spectra are done
+  }
+
+#pragma unroll
+  for (int o = 0; o < OUT; ++o) {
+    const int gi = tid + kCT * (o >> 3);
+    const int64_t f = out_f(gi, o & 7);
+    const double vx = kF32 ? (double)qh[o][0] + (double)ql[o][0] : qd[o][0];
+    const double vy = kF32 ? (double)qh[o][QC - 1] + (double)ql[o][QC - 1] : qd[o][QC - 1];
+    if (kFFT) partC[f] = make_double2(vx, vy);
+    else partR[f] = vx;
+  }
+  }  // item loop
+}
+
+// ------------------------------------------------------------------ host
+static int cl_logL(int variant, bool f32) { return (variant == kVariantFFT && !f32) ? 12 : 13; }
+
+bool sketch_cluster_applicable(int variant, bool f32, int b) {
+  const int logL = cl_logL(variant, f32);
+  int log2b = 0;
+  while ((1 << log2b) < b) ++log2b;
+  return log2b - logL >= 3 && log2b <= 19;  // R >= 8; DIF twiddle table covers b <= 2^19
+}
+
+template <int V, typename Real, typename CodeT>
+static void cl_kernel_attrs(size_t smem) {
+  CMM_CUDA(cudaFuncSetAttribute(k_sketch_cluster<V, Real, CodeT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CMM_CUDA(cudaFuncSetAttribute(k_sketch_cluster<V, Real, CodeT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+}
+
+static size_t cl_smem(int variant, bool f32, bool u16, int64_t SA, int64_t SB) {
+  const int L = 1 << cl_logL(variant, f32);
+  const size_t real = f32 ? 4 : 8, cpx = 2 * real;
+  size_t s;
+  if (variant == kVariantFFT) {
+    const size_t pl = f32 ? (size_t)L + L / 16 : (size_t)L + L / 8;
+    s = pl * cpx + (size_t)L * cpx + (1024 + 512) * cpx + 1184 * cpx;
+  } else {
+    const size_t pl = f32 ? (size_t)L + L / 32 : (size_t)L + L / 16;
+    s = 2 * pl * real;
+  }
+  s += 32 * real;
+  s += (size_t)(SA + SB) * (u16 ? 2 : 4);
+  return s;
+}
+
+template <int V, typename Real, typename CodeT>
+static void cl_launch(const ClArgs& a, dim3 grid, int R2, size_t smem, cudaStream_t s) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(kCT, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)R2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  CMM_CUDA(cudaLaunchKernelEx(&cfg, k_sketch_cluster<V, Real, CodeT>, a));
+}
+
+template <int V, typename Real, typename CodeT>
+static int cl_max_clusters(int R2, size_t smem) {
+  cl_kernel_attrs<V, Real, CodeT>(smem);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)R2, 1, 1);
+  cfg.blockDim = dim3(kCT, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)R2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, k_sketch_cluster<V, Real, CodeT>, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+// Chooses R2 in {16, 8} and the k-group count G from the number of
+// co-resident clusters NC: the grid holds NC persistent clusters that share
+// the R1 * d * G work items round-robin; the estimate ceil(items/NC)/G is
+// minimised (ties to R2 = 16: less scatter redundancy, fewer items).
+ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, int64_t est_slots) {
+  ClusterPlan C;
+  C.logL = cl_logL(variant, f32);
+  C.log2b = 0;
+  while ((1 << C.log2b) < b) ++C.log2b;
+  const int logR = C.log2b - C.logL;
+  double best = 1e300;
+  for (int logR2 : {4, 3}) {
+    if (logR2 > logR) continue;
+    const int R2 = 1 << logR2, R1 = 1 << (logR - logR2);
+    const size_t smem = cl_smem(variant, f32, true, est_slots, est_slots);
+    int mx;
+    if (variant == kVariantFFT)
+      mx = f32 ? cl_max_clusters<0, float, uint16_t>(R2, smem) : cl_max_clusters<0, double, uint16_t>(R2, smem);
+    else
+      mx = f32 ? cl_max_clusters<1, float, uint16_t>(R2, smem) : cl_max_clusters<1, double, uint16_t>(R2, smem);
+    if (mx <= 0) continue;
+    const int64_t base = (int64_t)R1 * d;
+    for (int64_t G = 1; G <= 64; ++G) {
+      if (G > 1 && G > n_inner) break;
+      if (base * G > 65535) break;
+      const int64_t items = base * G;
+      const int64_t nc = items < mx ? items : mx;
+      // per-cluster load in units of one (r1, t) over all k; scatter cost ~R1
+      const double load = (double)((items + nc - 1) / nc) / (double)G * (1.0 + 0.05 * R1);
+      if (load < best - 1e-9) {
+        best = load;
+        C.logR2 = logR2;
+        C.logR1 = logR - logR2;
+        C.G = (int)G;
+        C.max_clusters = (int)nc;
+      }
+    }
+  }
+  if (best >= 1e299) throw unsupported("no cluster configuration fits this device");
+  if (getenv("CMM_DEBUG"))
+    fprintf(stderr, "[cmm] cluster plan: b=%d L=%d R1=%d R2=%d G=%d clusters=%d\n", b, 1 << C.logL,
+            1 << C.logR1, 1 << C.logR2, C.G, C.max_clusters);
+  return C;
+}
+
+bool cluster_smem_fits(int variant, bool f32, const SlabPlan& P) {
+  return cl_smem(variant, f32, P.u16, P.EA, P.EB) <= 227 * 1024;
+}
+
+void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const SlabPlan& P,
+                           const void* dMatA, const void* dMatB, int64_t kc, const int* dScaleExp,
+                           int64_t k0, const double2* dTw, void* dPartial, int d, int accumulate,
+                           cudaStream_t s) {
+  ClArgs a;
+  a.matA = dMatA;
+  a.matB = dMatB;
+  a.codeA = P.codeA.ptr;
+  a.codeB = P.codeB.ptr;
+  a.countA = P.countA.as<uint32_t>();
+  a.countB = P.countB.as<uint32_t>();
+  a.scale_exp = dScaleExp;
+  a.tw = dTw;
+  a.partial = dPartial;
+  a.SA = P.EA;  // compact segments
+  a.SB = P.EB;
+  a.kc = kc;
+  a.k0 = k0;
+  a.d = d;
+  a.log2b = C.log2b;
+  a.logR1 = C.logR1;
+  a.logR2 = C.logR2;
+  a.G = C.G;
+  a.accumulate = accumulate;
+  const int R2 = 1 << C.logR2, R1 = 1 << C.logR1;
+  const size_t smem = cl_smem(variant, f32, P.u16, a.SA, a.SB);
+  if (smem > 227 * 1024) throw unsupported("cluster sketch: residue segments too large for shared memory");
+  (void)R1;
+  const dim3 grid((unsigned)R2, (unsigned)C.max_clusters, 1);
+  ProfScope prof("sketch", s);
+  count_launch();
+#define CMM_CL(V, T, CT)                       \
+  do {                                          \
+    cl_kernel_attrs<V, T, CT>(smem);            \
+    cl_launch<V, T, CT>(a, grid, R2, smem, s);  \
+  } while (0)
+  if (variant == kVariantFFT) {
+    if (f32) { if (P.u16) CMM_CL(0, float, uint16_t); else CMM_CL(0, float, uint32_t); }
+    else { if (P.u16) CMM_CL(0, double, uint16_t); else CMM_CL(0, double, uint32_t); }
+  } else {
+    if (f32) { if (P.u16) CMM_CL(1, float, uint16_t); else CMM_CL(1, float, uint32_t); }
+    else { if (P.u16) CMM_CL(1, double, uint16_t); else CMM_CL(1, double, uint32_t); }
+  }
+#undef CMM_CL
+  CMM_CUDA(cudaGetLastError());
+}
+
+}  // namespace cmm

@@ -641,7 +641,7 @@ void launch_materialize_f32(const SlabPlan& P, const float* dAT, const float* dB
   const int64_t nmax = P.n_a > P.n_b ? P.n_a : P.n_b;
   const size_t smem = (size_t)nmax * 4;
   const int stage = smem <= 200 * 1024 ? 1 : 0;
-  const int64_t SA = (int64_t)P.EA * kPlanThreads, SB = (int64_t)P.EB * kPlanThreads;
+  const int64_t SA = P.slots_a(), SB = P.slots_b();
   ProfScope prof("materialize", s);
   count_launch();
   if (stage)

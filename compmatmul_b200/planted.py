@@ -12,6 +12,7 @@ reference binding requires (compmatmul.cpp:65-73).
 The named workloads follow the benchmark configurations of this project:
   config1   n=512,   K=32,   FFT,  b=4096,  d=5   (CPU-runnable case)
   config2   n=4096 / 16384, K=256, b=2^16, d=9, FFT and FWHT, FP64
+  config3   n=16384, K=1024, b=2^18, d=9, FP32 inputs (mixed precision)
 """
 from __future__ import annotations
 
@@ -23,6 +24,8 @@ WORKLOADS = {
                           seed=9002),
     "config2_n16384": dict(n=16384, K=256, b=1 << 16, d=9, variants=("fft", "fwht"),
                            gen_seed=1638401, seed=9003),
+    "config3": dict(n=16384, K=1024, b=1 << 18, d=9, variants=("fft", "fwht"), gen_seed=1638403,
+                    seed=9004, dtype="float32"),
 }
 
 
