@@ -35,7 +35,7 @@ EXPORTED = [
     "cmm_dev_compressed_product", "cmm_dev_decompress_dense", "cmm_dev_matmul", "cmm_dev_topk",
     "cmm_dev_gemm", "cmm_profile_enable", "cmm_profile_reset", "cmm_profile_read",
     "cmm_launch_count", "cmm_dev_compressed_product_f32", "cmm_dev_matmul_f32",
-    "cmm_compressed_product_f32", "cmm_matmul_f32",
+    "cmm_compressed_product_f32", "cmm_matmul_f32", "cmm_dev_compressed_product_noalloc",
 ]
 
 
@@ -70,6 +70,8 @@ def lib():
     L.cmm_gemm.argtypes = [i64, i64, i64, dp, dp, dp]
     L.cmm_hash_codes.argtypes = [i32, i32, i32, u64, i32, i64, vp]
     L.cmm_dev_compressed_product.argtypes = [i32, i32, i64, i64, i64, dp, dp, i32, i32, u64, dp, vp]
+    L.cmm_dev_compressed_product_noalloc.argtypes = [i32, i32, i64, i64, i64, dp, dp, i32, i32, u64,
+                                                     dp, vp]
     L.cmm_dev_decompress_dense.argtypes = [i32, i32, i64, i64, i32, i32, u64, dp, dp, vp]
     L.cmm_dev_matmul.argtypes = [i32, i32, i64, i64, i64, dp, dp, dp, i32, i32, u64, vp]
     L.cmm_dev_topk.argtypes = [dp, i64, i64, i32, vp, vp, dp, vp]

@@ -469,6 +469,68 @@ int cmm_dev_compressed_product(int variant, int hash_kind, int64_t n_a, int64_t 
   });
 }
 
+// Allocation-free twin of cmm_dev_compressed_product: the slab pipeline
+// (hash codes -> row balance -> k_sketch_{fft,fwht} -> k-group reduction +
+// inverse) with every intermediate carved from the static device scratch.
+// The sizes are checked against the scratch before any CUDA call.
+int cmm_dev_compressed_product_noalloc(int variant, int hash_kind, int64_t n_a, int64_t n_inner,
+                                       int64_t n_b, const double* dAT, const double* dB, int d,
+                                       int b, uint64_t seed, double* dP, void* stream) {
+  return guarded([&] {
+    check_params(variant, hash_kind, d, b);
+    check_sizes(n_a, n_inner, n_b);
+    const bool fft = variant == kVariantFFT;
+    const size_t elem = fft ? 16 : 8;
+    const size_t db = (size_t)d * (size_t)b;
+    auto a256 = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    size_t off = 0;
+    auto take = [&](size_t n) { const size_t o = off; off += a256(n); return o; };
+    const size_t set = hash_param_bytes(hash_kind) * (size_t)d;
+    const size_t o_blob = take(4 * set);
+    const size_t o_ca = take((size_t)d * (size_t)n_a * 4);
+    const size_t o_cb = take((size_t)d * (size_t)n_b * 4);
+    const size_t o_scale = take(fft ? (size_t)(n_inner > 0 ? n_inner : 1) * 4 : 0);
+    const size_t o_tw = take((size_t)b * 16);
+    const size_t o_work = take(2 * db * elem);
+    const size_t o_part = off;
+    if (o_part > kNoAllocScratchBytes || kNoAllocScratchBytes - o_part < db * elem)
+      throw unsupported("cmm_dev_compressed_product_noalloc: this product needs " +
+                        std::to_string(o_part + db * elem) + " bytes of scratch; the static scratch holds " +
+                        std::to_string(kNoAllocScratchBytes) +
+                        " bytes (use cmm_dev_compressed_product for larger sizes)");
+    const int64_t g_fit = (int64_t)((kNoAllocScratchBytes - o_part) / (db * elem));
+
+    cudaStream_t s = (cudaStream_t)stream;
+    SketchPlan P = plan_sketch(variant, n_a, n_inner, n_b, d, b, num_sms());
+    if (P.G > g_fit) P.G = (int)g_fit;
+    uint8_t* base = static_cast<uint8_t*>(noalloc_scratch());
+    const SketchParams sp = make_sketch_params(hash_kind, d, b, seed);
+    CMM_CUDA(cudaMemcpyAsync(base + o_blob, sp.blob.data(), sp.blob.size(), cudaMemcpyHostToDevice, s));
+    uint32_t* ca = reinterpret_cast<uint32_t*>(base + o_ca);
+    uint32_t* cb = reinterpret_cast<uint32_t*>(base + o_cb);
+    launch_hash_codes(hash_kind, base + o_blob, base + o_blob + 2 * set, d, sp.log2b, n_a, ca, s);
+    launch_hash_codes(hash_kind, base + o_blob + set, base + o_blob + 3 * set, d, sp.log2b, n_b, cb, s);
+    {
+      // w[j] = exp(-2 pi i j / b) in long double, as the cached table
+      std::vector<double2> h((size_t)b);
+      const long double two_pi = 6.283185307179586476925286766559005768L;
+      for (int j = 0; j < b; ++j) {
+        const long double a = -two_pi * (long double)j / (long double)b;
+        h[(size_t)j] = make_double2((double)cosl(a), (double)sinl(a));
+      }
+      CMM_CUDA(cudaMemcpyAsync(base + o_tw, h.data(), sizeof(double2) * (size_t)b,
+                               cudaMemcpyHostToDevice, s));
+    }
+    const double2* tw = reinterpret_cast<const double2*>(base + o_tw);
+    int* scale = fft ? reinterpret_cast<int*>(base + o_scale) : nullptr;
+    if (fft) launch_row_scale(dAT, dB, n_a, n_inner, n_b, scale, s);
+    void* part = base + o_part;
+    CMM_CUDA(cudaMemsetAsync(part, 0, (size_t)P.G * db * elem, s));  // k-group partials start at zero
+    launch_sketch_accumulate(P, dAT, dB, ca, cb, scale, tw, part, s);
+    launch_finalize(P, part, tw, base + o_work, dP, s);
+  });
+}
+
 int cmm_dev_decompress_dense(int variant, int hash_kind, int64_t n_a, int64_t n_b, int d, int b,
                              uint64_t seed, const double* dP, double* dC, void* stream) {
   return guarded([&] {

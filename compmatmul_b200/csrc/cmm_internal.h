@@ -89,6 +89,10 @@ constexpr int kFftLmaxLog = 12;   // 4096 complex FP64 (64 KB) + accumulator
 constexpr int kFwhtLmaxLog = 13;  // 8192 real FP64 x 2 (128 KB) + accumulator
 constexpr int kMaxLog2B = 24;     // b <= 2^24 (R = b/L <= 4096)
 
+// Static scratch of the allocation-free entry point (32 MiB per device).
+constexpr size_t kNoAllocScratchBytes = (size_t)32 << 20;
+void* noalloc_scratch();  // its device address, looked up once per device
+
 struct SketchPlan {
   int variant, d, b, log2b;
   int logL, L;       // sub-transform length L = b / R

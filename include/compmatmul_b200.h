@@ -113,6 +113,37 @@ int cmm_dev_compressed_product(int variant, int hash_kind, int64_t n_a, int64_t 
                                int64_t n_b, const double* dAT, const double* dB, int d, int b,
                                uint64_t seed, double* dP, void* stream);
 
+/* Allocation-free twin of cmm_dev_compressed_product; it has no counterpart
+ * in the reference (which allocates its sketches on the host heap,
+ * matmul_fft.hpp / matmul_fwht.hpp).  For callers that cannot call
+ * cudaMalloc: a plugin whose host framework owns all device memory and
+ * forbids allocation after set-up, or a serving loop whose pool already
+ * holds the HBM (cudaMalloc would fail or break its budget, and cudaFree
+ * synchronises the whole device, stalling every other stream).
+ *   - It calls no cudaMalloc / cudaMallocAsync / cudaFree and no allocating
+ *     library routine: every intermediate (hash parameters, codes, row
+ *     scales, twiddles, k-group partials, inverse work) lives in one
+ *     file-scope device array of CMM_NOALLOC_SCRATCH_BYTES per device.
+ *     The host side draws the hash parameters and twiddles into ordinary
+ *     host memory and copies them in with cudaMemcpyAsync.
+ *   - Scratch needed, in bytes (each term rounded up to 256):
+ *       4 * d * param_bytes(hash) + 4 * d * n_a + 4 * d * n_b
+ *       + 4 * n_inner (FFT only) + 16 * b + 2 * d * b * e + d * b * e,
+ *     e = 16 (FFT) or 8 (FWHT); param_bytes = 8 (MS), 16 (MAS), 4096
+ *     (tab8), 524288 (tab16).  Larger products return CMM_ERR_UNSUPPORTED
+ *     before any CUDA call, with the bytes needed in cmm_last_error().
+ *   - The first call on a device looks up the scratch address
+ *     (cudaGetSymbolAddress, once per device); make that first call before
+ *     any stream capture begins.
+ *   - The k-group partials are cleared on every call; all other scratch is
+ *     fully written before it is read.
+ *   - Calls that overlap in time on one device (other streams, other host
+ *     threads) race on the one scratch array: serialise them. */
+#define CMM_NOALLOC_SCRATCH_BYTES (32u << 20)
+int cmm_dev_compressed_product_noalloc(int variant, int hash_kind, int64_t n_a, int64_t n_inner,
+                                       int64_t n_b, const double* dAT, const double* dB, int d,
+                                       int b, uint64_t seed, double* dP, void* stream);
+
 /* Dense median decompression of dP into dC (n_a x n_b FP64). */
 int cmm_dev_decompress_dense(int variant, int hash_kind, int64_t n_a, int64_t n_b, int d, int b,
                              uint64_t seed, const double* dP, double* dC, void* stream);
