@@ -52,6 +52,15 @@ def parse():
     return ap.parse_args()
 
 
+# DRAM traffic of one sketch-kernel launch relative to its algorithmic bytes
+# (the row pairs it must read once per repetition), from one ncu capture of
+# the same kernel on a small case: dram__bytes_read.sum + dram__bytes_write.sum
+# over d * k_chunk * (n_a + n_b) * element bytes, scaled to a full launch by
+# the units it processes (the row reads dominate and grow in proportion).
+# Source: profiles/k_sketch_cluster_fft_small.md (filled in from a capture).
+TRAFFIC_RATIO = {}
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -254,7 +263,9 @@ def main():
     launches = L.cmm_launch_count() - launches0
     L.cmm_profile_enable(0)
     total_ms = ev0.elapsed_time(ev1)
-    fam = {f: cmb.profile_read(f) for f in ("hash", "scale", "sketch", "finalize", "decompress", "topk")}
+    fam = {f: cmb.profile_read(f) for f in ("hash", "scale", "plan", "materialize", "sketch",
+                                             "finalize", "decompress", "topk")}
+    sketch_kernel = L.cmm_last_sketch_kernel().decode()
     t = torch.tensor([total_ms], dtype=torch.float64, device=dv)
     if world > 1:
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -300,14 +311,24 @@ def main():
         fp64_ms = (time.perf_counter() - tf0) / args.compare_fp64 * 1e3
         del dAT64, dB64
 
-    # roofline of the dominant kernel (sketch)
+    # roofline of the dominant kernel (the sketch kernel): one launch covers a
+    # chunk of the inner indices; per launch it must read the chunk's row
+    # pairs once per repetition (d * k_chunk * (n_a + n_b) elements) and does
+    # the chunk's share of the transform arithmetic
     sk_ms, sk_n = fam["sketch"]
     sk_launch_ms = sk_ms / max(1, sk_n)
+    chunks = max(1, sk_n // max(1, args.steps))  # launches per product
     esz = 4.0 if mixed else 8.0
-    alg_bytes = esz * n * (n + n)  # reads of AT and B per launch
+    alg_bytes = esz * d * n * (n + n) / chunks
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (sk_launch_ms / 1e3) / 1e9
-    flops = fft_flops(n, n, n, d, b) if variant == "fft" else fwht_ops(n, n, n, d, b)
+    flops = (fft_flops(n, n, n, d, b) if variant == "fft" else fwht_ops(n, n, n, d, b)) / chunks
+    ratio = TRAFFIC_RATIO.get((sketch_kernel, variant, "f32" if mixed else "f64"))
+    import ctypes as C
+    fma_peak = None
+    tf = C.c_double(0.0)
+    if L.cmm_probe_fma_tflops(0 if mixed else 1, C.byref(tf)) == 0:
+        fma_peak = tf.value
 
     if rank != 0:
         if world > 1:
@@ -331,10 +352,17 @@ def main():
         "dtype": "f32 (mixed: FP32 transforms, FP64 reduction)" if mixed else "f64",
         "data": "synthetic", "config": config,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "kernel": "k_sketch_fft" if variant == "fft" else "k_sketch_fwht",
-                     "peak_source": peak_kind, "launch_ms": sk_launch_ms,
+                     "frac": achieved / peak, "traffic": ratio * alg_bytes if ratio else None,
+                     "traffic_source": "ncu small case scaled by units" if ratio else None,
+                     "kernel": f"sketch ({sketch_kernel})", "peak_source": peak_kind,
+                     "launch_ms": sk_launch_ms, "launches_per_product": chunks,
                      "algorithmic_bytes_per_launch": alg_bytes,
-                     "fp64_tflops_achieved": flops / (sk_launch_ms / 1e3) / 1e12},
+                     "binding": {"bound": "fp32" if mixed else "fp64",
+                                 "achieved": flops / (sk_launch_ms / 1e3) / 1e12,
+                                 "peak": fma_peak, "unit": "TFLOP/s",
+                                 "frac": (flops / (sk_launch_ms / 1e3) / 1e12 / fma_peak) if fma_peak else None,
+                                 "peak_source": "measured FMA loop (cmm_probe_fma_tflops)",
+                                 "flops_per_launch": flops}},
         "kernel_ms_per_step": {k: v[0] / max(1, args.steps) for k, v in fam.items()},
         "e2e": {"value": e2e_value, "unit": "products/s", "h2d_bytes_per_step": int(2 * esz * n * n),
                 "d2h_bytes_per_step": int(8 * n * n)},

@@ -36,6 +36,7 @@ EXPORTED = [
     "cmm_dev_gemm", "cmm_profile_enable", "cmm_profile_reset", "cmm_profile_read",
     "cmm_launch_count", "cmm_dev_compressed_product_f32", "cmm_dev_matmul_f32",
     "cmm_compressed_product_f32", "cmm_matmul_f32", "cmm_dev_compressed_product_noalloc",
+    "cmm_last_sketch_kernel", "cmm_probe_fma_tflops",
 ]
 
 
@@ -62,6 +63,8 @@ def lib():
     vp, dp = _C.c_void_p, _C.c_void_p
     L.cmm_last_error.restype = _C.c_char_p
     L.cmm_version.restype = _C.c_char_p
+    L.cmm_last_sketch_kernel.restype = _C.c_char_p
+    L.cmm_probe_fma_tflops.argtypes = [_C.c_int, _C.POINTER(_C.c_double)]
     L.cmm_device_count.restype = i32
     L.cmm_max_buckets.restype = i32
     L.cmm_matmul.argtypes = [i32, i32, i64, i64, i64, dp, dp, dp, i32, i32, i32, u64]
@@ -86,7 +89,7 @@ def lib():
     L.cmm_profile_read.argtypes = [_C.c_char_p, _C.POINTER(_C.c_double), _C.POINTER(i64)]
     L.cmm_launch_count.restype = i64
     for name in EXPORTED:
-        if name not in ("cmm_last_error", "cmm_version", "cmm_profile_enable",
+        if name not in ("cmm_last_error", "cmm_version", "cmm_profile_enable", "cmm_last_sketch_kernel",
                         "cmm_profile_reset", "cmm_launch_count"):
             getattr(L, name).restype = i32
     _lib = L

@@ -226,6 +226,7 @@ static void sketch_device(int variant, const SketchParams& sp, const Codes& code
   SlabPlan plan;
   if (n_inner > 0 && try_cluster_plan(variant, false, codes, n_a, n_b, n_inner, sp, C, plan, s)) {
     // residue plan + per-chunk materialized rows + cluster kernels
+    set_sketch_kernel("cluster");
     const int64_t SA = plan.slots_a(), SB = plan.slots_b();
     const size_t per_row = (size_t)sp.d * (size_t)(SA + SB) * 8;
     int64_t kc = (int64_t)(materialize_budget() / per_row);
@@ -245,6 +246,7 @@ static void sketch_device(int variant, const SketchParams& sp, const Codes& code
   }
   if (n_inner > 0 && sketch_v1_applicable(variant, sp.b, n_a, n_b)) {
     // bucket-sorted plan + per-chunk materialized rows + v1 kernels
+    set_sketch_kernel("slab");
     const SketchPlan P = plan_sketch_v1(variant, n_a, n_inner, n_b, sp.d, sp.b, num_sms());
     SlabPlan plan = make_slab_plan(codes.a.as<uint32_t>(), codes.b.as<uint32_t>(), n_a, n_b, sp.d,
                                    sp.b, P.logL, s);
@@ -266,6 +268,7 @@ static void sketch_device(int variant, const SketchParams& sp, const Codes& code
     return;
   }
   const SketchPlan P = plan_sketch(variant, n_a, n_inner, n_b, sp.d, sp.b, num_sms());
+  set_sketch_kernel("small-b");
   DevBuf partial((size_t)P.G * sp.d * (size_t)sp.b * elem, s);
   launch_sketch_accumulate(P, dAT, dB, codes.a.as<uint32_t>(), codes.b.as<uint32_t>(),
                            scale.as<int>(), tw, partial.ptr, s);
@@ -293,6 +296,7 @@ static void sketch_device_mixed(int variant, const SketchParams& sp, const Codes
   ClusterPlan Cp;
   SlabPlan cplan;
   if (try_cluster_plan(variant, true, codes, n_a, n_b, n_inner, sp, Cp, cplan, s)) {
+    set_sketch_kernel("cluster");
     SlabPlan& plan = cplan;
     const int64_t SA = plan.slots_a(), SB = plan.slots_b();
     const size_t per_row = (size_t)sp.d * (size_t)(SA + SB) * 4;
@@ -312,6 +316,7 @@ static void sketch_device_mixed(int variant, const SketchParams& sp, const Codes
     return;
   }
   const SketchPlan P = plan_sketch_mixed(variant, n_a, n_inner, n_b, sp.d, sp.b, num_sms());
+  set_sketch_kernel("slab-mixed");
   SlabPlan plan = make_slab_plan(codes.a.as<uint32_t>(), codes.b.as<uint32_t>(), n_a, n_b, sp.d,
                                  sp.b, P.logL, s);
   const int64_t SA = (int64_t)plan.EA * kPlanThreads, SB = (int64_t)plan.EB * kPlanThreads;
@@ -347,6 +352,9 @@ static std::map<std::string, FamilyTimes>& prof_table() {
 }
 
 void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+static thread_local std::string g_sketch_kernel;
+void set_sketch_kernel(const char* name) { g_sketch_kernel = name; }
 
 void prof_begin(const char* family, cudaStream_t s) {
   if (!g_prof.load()) return;
@@ -455,6 +463,15 @@ int cmm_profile_read(const char* family, double* total_ms, int64_t* launches) {
 }
 
 int64_t cmm_launch_count(void) { return g_launches.load(); }
+
+const char* cmm_last_sketch_kernel(void) { return g_sketch_kernel.c_str(); }
+
+int cmm_probe_fma_tflops(int fp64, double* tflops) {
+  return guarded([&] {
+    if (!tflops) throw invalid_argument("tflops must not be null");
+    *tflops = probe_fma_tflops(fp64 != 0, host_stream());
+  });
+}
 
 int cmm_dev_compressed_product(int variant, int hash_kind, int64_t n_a, int64_t n_inner,
                                int64_t n_b, const double* dAT, const double* dB, int d, int b,

@@ -215,6 +215,8 @@ int num_sms();
 void prof_begin(const char* family, cudaStream_t s);
 void prof_end(const char* family, cudaStream_t s);
 void count_launch(int n = 1);
+void set_sketch_kernel(const char* name);  // recorded for cmm_last_sketch_kernel
+double probe_fma_tflops(bool fp64, cudaStream_t s);
 struct ProfScope {
   const char* fam;
   cudaStream_t s;

@@ -186,8 +186,8 @@ int cmm_matmul_f32(int variant, int hash_kind, int64_t n_a, int64_t n_inner, int
 /* ---------------------------------------------------------------------
  * Instrumentation for benchmarks (no reference twin).  When enabled, every
  * kernel launch of a family is bracketed by CUDA events recorded on the
- * stream it is launched on.  Families: "hash", "scale", "sketch",
- * "finalize", "decompress", "topk", "gemm".
+ * stream it is launched on.  Families: "hash", "scale", "plan",
+ * "materialize", "sketch", "finalize", "decompress", "topk", "gemm".
  * ------------------------------------------------------------------- */
 void cmm_profile_enable(int on);
 void cmm_profile_reset(void);
@@ -196,6 +196,13 @@ void cmm_profile_reset(void);
 int cmm_profile_read(const char* family, double* total_ms, int64_t* launches);
 /* Kernels launched by this library since load (always counted). */
 int64_t cmm_launch_count(void);
+/* Name of the sketch kernel family the last compressed product on this host
+ * thread ran ("cluster", "slab", "slab-mixed", "small-b"); "" before any. */
+const char* cmm_last_sketch_kernel(void);
+/* Measured FMA throughput of the current device in TFLOP/s (2 flops per
+ * FMA; FP64 if fp64 != 0, else FP32), from a register-resident FMA loop
+ * timed with CUDA events: the arithmetic roofline's denominator. */
+int cmm_probe_fma_tflops(int fp64, double* tflops);
 
 #ifdef __cplusplus
 }
