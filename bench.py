@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--n", type=int, default=0, help="override the workload size (profiling)")
     ap.add_argument("--compare-fp64", type=int, default=0,
                     help="also time N steps of the plain FP64 path on the same inputs")
+    ap.add_argument("--batch-count", type=int, default=256, help="products of the config4 batch")
+    ap.add_argument("--batch-tune", type=int, default=1, help="config4: run the autotuner (0: defaults)")
     ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"],
                     help="fp64 = plain path; mixed = FP32 inputs (default for config3)")
     return ap.parse_args()
@@ -167,12 +169,251 @@ def cpu_reference_sample(AT, B, n, d, b, variant, seed, budget_s):
     return per_product, thr, sample
 
 
+# ------------------------------------------------- batched products (config 4)
+def product_flops(s):
+    f = fft_flops if s["variant"] == "fft" else fwht_ops
+    return f(s["m"], s["n"], s["p"], s["d"], s["b"])
+
+
+def bench_batch(args, world, rank, local):
+    """Config 4: 256 uneven planted products (FP32 inputs) as one batch plan:
+    one persistent sketch launch over a work queue, the whole batch replayed
+    from a CUDA graph; a step is one run of all products (sketches + dense
+    median estimates).  Compared with the plain FP64 path on the same
+    inputs, both batched and as one cmm_dev_matmul call per product."""
+    from compmatmul_b200.planted import batch_shapes, planted_problem_device
+    count = args.batch_count
+    shapes = batch_shapes(count=count, seed=4004 + 1000 * rank)
+    config = {"workload": f"config4: {count} planted products m x n x p, each dimension log-uniform in "
+                          f"[256, 4096], FP32 noise N(0,0.01^2) + K=max(8,m/64) planted +10/+10, "
+                          f"b = next pow2 >= 256 K, d in {{5,7,9}}, FFT/FWHT 50/50; sketch + dense median "
+                          f"estimate per product",
+              "products": count, "l2": "inputs (sum 4 n (m+p) bytes) larger than L2, no flush"}
+    flops_total = sum(product_flops(s) for s in shapes)
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from oracle.oracle import RefLib
+        from compmatmul_b200.planted import planted_problem
+        rl = RefLib()
+        t_used, f_used, done = 0.0, 0.0, 0
+        for s in shapes:
+            AT, B, _ = planted_problem(s["m"], s["n"], s["p"], s["K"], s["gen_seed"], dtype=np.float32)
+            t0 = time.perf_counter()
+            rl.matmul(s["variant"], None, AT.astype(np.float64), B.astype(np.float64), s["d"], s["b"], s["seed"])
+            t_used += time.perf_counter() - t0
+            f_used += product_flops(s)
+            done += 1
+            if t_used > args.cpu_seconds:
+                break
+        sec = t_used * flops_total / f_used  # one batch, scaled by modelled work
+        val = count / sec
+        sample = (f"reference CPU path (headers compiled with shims, {rl.num_threads()} threads, FP64 on the "
+                  f"FP32-valued inputs) on the first {done} of {count} products ({t_used:.1f} s), scaled to the "
+                  f"batch by the modelled flops")
+        print(json.dumps({"metric": METRIC, "value": val, "unit": "products/s", "impl": "reference",
+                          "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+                          "cpu_baseline": {"value": val, "unit": "products/s", "cores": rl.num_threads(),
+                                           "kind": "reference", "sample": sample},
+                          "e2e": {"value": val, "unit": "products/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
+
+    import ctypes as C
+    import torch
+    import compmatmul_b200 as cmb
+    from compmatmul_b200 import device as dev
+    from compmatmul_b200.batch import BatchPlan
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    L = cmb.lib()
+    prods, planted = [], []
+    for s in shapes:
+        AT, B, pl = planted_problem_device(s["m"], s["n"], s["p"], s["K"], s["gen_seed"], "float32")
+        prods.append(dict(AT=AT, B=B, d=s["d"], b=s["b"], seed=s["seed"], variant=s["variant"]))
+        planted.append(pl)
+    t0 = time.perf_counter()
+    plan = BatchPlan(prods, f32=True, tune=bool(args.batch_tune), dense=True)
+    plan_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        plan.run()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    clocks = ClockSampler(torch.cuda.current_device())
+    L.cmm_profile_reset()
+    L.cmm_profile_enable(1)
+    launches0 = L.cmm_launch_count()
+    barrier()
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        plan.run()
+    ev1.record()
+    barrier()
+    clk = clocks.stop()
+    launches = L.cmm_launch_count() - launches0
+    L.cmm_profile_enable(0)
+    total_ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * count * args.steps / (total_ms / 1e3)
+    info = plan.info()
+
+    # the persistent sketch kernel alone (its own run, events on the same stream)
+    ek0 = torch.cuda.Event(enable_timing=True)
+    ek1 = torch.cuda.Event(enable_timing=True)
+    L.cmm_profile_reset()
+    L.cmm_profile_enable(1)
+    ek0.record()
+    plan.run()
+    ek1.record()
+    torch.cuda.synchronize()
+    L.cmm_profile_enable(0)
+    batch_ms = cmb.profile_read("batch")[0]
+
+    # recovery: planted entries among each product's top-K estimates
+    rec = tot = 0
+    for q, (is_, ks, js), s in zip(plan.products, planted, shapes):
+        ti, tj, _ = dev.topk(q["C"], s["K"])
+        rec += len(set(zip(ti.tolist(), tj.tolist())) & set(zip(is_.tolist(), js.tolist())))
+        tot += s["K"]
+
+    # plain FP64 on the same inputs: batched, and one cmm_dev_matmul per product
+    fp64 = None
+    if args.compare_fp64:
+        prods64 = [dict(q, AT=q["AT"].double(), B=q["B"].double()) for q in prods]
+        plan64 = BatchPlan(prods64, f32=False, tune=True, dense=True)
+        for _ in range(2):
+            plan64.run()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.compare_fp64):
+            plan64.run()
+        e1.record()
+        torch.cuda.synchronize()
+        b64 = e0.elapsed_time(e1) / args.compare_fp64
+        outs = [torch.empty((q["AT"].shape[1], q["B"].shape[1]), dtype=torch.float64, device="cuda")
+                for q in prods64]
+        for q, o in zip(prods64, outs):  # warm
+            dev.matmul(q["AT"], q["B"], q["d"], q["b"], q["seed"], variant=q["variant"], out=o)
+        torch.cuda.synchronize()
+        e0.record()
+        for q, o in zip(prods64, outs):
+            dev.matmul(q["AT"], q["B"], q["d"], q["b"], q["seed"], variant=q["variant"], out=o)
+        e1.record()
+        torch.cuda.synchronize()
+        single64 = e0.elapsed_time(e1)
+        maxrel = {"fft": 0.0, "fwht": 0.0}
+        same_sets = 0
+        for q, q64, s in zip(plan.products, plan64.products, shapes):
+            ti, tj, tv = dev.topk(q64["C"], s["K"])
+            mi, mj, _ = dev.topk(q["C"], s["K"])
+            same_sets += set(zip(ti.tolist(), tj.tolist())) == set(zip(mi.tolist(), mj.tolist()))
+            got = q["C"][torch.as_tensor(ti, device="cuda"), torch.as_tensor(tj, device="cuda")].cpu().numpy()
+            err = float(np.max(np.abs(got - tv) / np.maximum(np.abs(tv), 1e-300)))
+            maxrel[s["variant"]] = max(maxrel[s["variant"]], err)
+        fp64 = {"batched_ms_per_step": b64, "single_product_calls_ms_per_step": single64,
+                "speedup_vs_batched_fp64": b64 / ms_per_step, "speedup_vs_single_fp64": single64 / ms_per_step,
+                "max_rel_err_recovered_vs_fp64": maxrel,
+                "same_recovered_sets_as_fp64": f"{same_sets}/{count}"}
+        plan64.close()
+        del prods64, outs
+
+    # end to end with host buffers: pinned inputs in, dense estimates out
+    hin = [(torch.empty_like(q["AT"], device="cpu").pin_memory(), torch.empty_like(q["B"], device="cpu").pin_memory())
+           for q in prods]
+    hout = [torch.empty_like(q["C"], device="cpu").pin_memory() for q in plan.products]
+    for (ha, hb), q in zip(hin, prods):
+        ha.copy_(q["AT"])
+        hb.copy_(q["B"])
+    h2d = sum(ha.numel() * 4 + hb.numel() * 4 for ha, hb in hin)
+    d2h = sum(o.numel() * 8 for o in hout)
+    e2e_steps = max(1, args.e2e_steps)
+    barrier()
+    te0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for (ha, hb), q in zip(hin, prods):
+            q["AT"].copy_(ha, non_blocking=True)
+            q["B"].copy_(hb, non_blocking=True)
+        plan.run()
+        for o, q in zip(hout, plan.products):
+            o.copy_(q["C"], non_blocking=True)
+        torch.cuda.synchronize()
+    barrier()
+    e2e_s = (time.perf_counter() - te0) / e2e_steps
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = world * count / float(te.item())
+
+    fma = C.c_double(0.0)
+    fma_peak = fma.value if L.cmm_probe_fma_tflops(0, C.byref(fma)) == 0 else None
+    alg_bytes = sum(4.0 * s["d"] * s["n"] * (s["m"] + s["p"]) for s in shapes)
+    peak, peak_kind = measured_peaks()
+    if rank != 0:
+        plan.close()
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": "products/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (mixed: FP32 transforms, FP64 reduction)", "data": "synthetic",
+        "config": config,
+        "roofline": {"bound": "hbm", "achieved": alg_bytes / (batch_ms / 1e3) / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": alg_bytes / (batch_ms / 1e3) / 1e9 / peak, "traffic": None,
+                     "kernel": "batch graph (persistent k_batch_sketch + per-product finalize/decompress)",
+                     "peak_source": peak_kind, "launch_ms": batch_ms, "algorithmic_bytes_per_launch": alg_bytes,
+                     "binding": {"bound": "fp32", "achieved": flops_total / (batch_ms / 1e3) / 1e12,
+                                 "peak": fma_peak, "unit": "TFLOP/s",
+                                 "frac": (flops_total / (batch_ms / 1e3) / 1e12 / fma_peak) if fma_peak else None,
+                                 "peak_source": "measured FMA loop (cmm_probe_fma_tflops)",
+                                 "flops_per_launch": flops_total}},
+        "e2e": {"value": e2e_value, "unit": "products/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "recovered_planted": f"{rec}/{tot}",
+        "batch": {"items": info["items"], "ctas": info["ctas"], "launches_per_run": info["launches"],
+                  "plan_and_tune_s": plan_s},
+        "cpu_baseline": None,
+    }
+    if fp64 is not None:
+        line["plain_fp64_same_inputs"] = fp64
+    print(json.dumps(line), flush=True)
+    plan.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 # --------------------------------------------------------------- main
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "config4":
+        bench_batch(args, world, rank, local)
+        return
     from compmatmul_b200.planted import WORKLOADS, planted_problem
     w = dict(WORKLOADS[args.workload])
     if args.n:

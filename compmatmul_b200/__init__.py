@@ -36,7 +36,8 @@ EXPORTED = [
     "cmm_dev_gemm", "cmm_profile_enable", "cmm_profile_reset", "cmm_profile_read",
     "cmm_launch_count", "cmm_dev_compressed_product_f32", "cmm_dev_matmul_f32",
     "cmm_compressed_product_f32", "cmm_matmul_f32", "cmm_dev_compressed_product_noalloc",
-    "cmm_last_sketch_kernel", "cmm_probe_fma_tflops",
+    "cmm_last_sketch_kernel", "cmm_probe_fma_tflops", "cmm_batch_create", "cmm_batch_run",
+    "cmm_batch_info", "cmm_batch_config", "cmm_batch_destroy",
 ]
 
 
@@ -65,6 +66,12 @@ def lib():
     L.cmm_version.restype = _C.c_char_p
     L.cmm_last_sketch_kernel.restype = _C.c_char_p
     L.cmm_probe_fma_tflops.argtypes = [_C.c_int, _C.POINTER(_C.c_double)]
+    L.cmm_batch_create.argtypes = [vp, i32, i32, i32, _C.POINTER(_C.c_void_p)]
+    L.cmm_batch_run.argtypes = [vp, vp]
+    L.cmm_batch_info.argtypes = [vp, _C.POINTER(_C.c_int64), _C.POINTER(_C.c_int), _C.POINTER(_C.c_int)]
+    L.cmm_batch_config.argtypes = [vp, i32, _C.POINTER(_C.c_int), _C.POINTER(_C.c_int),
+                                   _C.POINTER(_C.c_int), _C.POINTER(_C.c_int)]
+    L.cmm_batch_destroy.argtypes = [vp]
     L.cmm_device_count.restype = i32
     L.cmm_max_buckets.restype = i32
     L.cmm_matmul.argtypes = [i32, i32, i64, i64, i64, dp, dp, dp, i32, i32, i32, u64]

@@ -356,6 +356,8 @@ void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 static thread_local std::string g_sketch_kernel;
 void set_sketch_kernel(const char* name) { g_sketch_kernel = name; }
 
+bool prof_set(bool on) { return g_prof.exchange(on); }
+
 void prof_begin(const char* family, cudaStream_t s) {
   if (!g_prof.load()) return;
   std::lock_guard<std::mutex> g(g_prof_mu);
@@ -465,6 +467,31 @@ int cmm_profile_read(const char* family, double* total_ms, int64_t* launches) {
 int64_t cmm_launch_count(void) { return g_launches.load(); }
 
 const char* cmm_last_sketch_kernel(void) { return g_sketch_kernel.c_str(); }
+
+int cmm_batch_create(const cmm_batch_product* products, int count, int f32, int tune, void** handle) {
+  return guarded([&] {
+    if (!handle) throw invalid_argument("handle must not be null");
+    *handle = nullptr;
+    *handle = batch_create(products, count, f32 != 0, tune != 0);
+  });
+}
+
+int cmm_batch_run(void* handle, void* stream) {
+  return guarded([&] { batch_run(static_cast<BatchPlan*>(handle), (cudaStream_t)stream); });
+}
+
+int cmm_batch_info(void* handle, int64_t* items, int* ctas, int* launches) {
+  return guarded([&] { batch_info(static_cast<const BatchPlan*>(handle), items, ctas, launches); });
+}
+
+int cmm_batch_config(void* handle, int product, int* log2_slab, int* radix, int* groups, int* tuned) {
+  return guarded(
+      [&] { batch_config(static_cast<const BatchPlan*>(handle), product, log2_slab, radix, groups, tuned); });
+}
+
+int cmm_batch_destroy(void* handle) {
+  return guarded([&] { batch_destroy(static_cast<BatchPlan*>(handle)); });
+}
 
 int cmm_probe_fma_tflops(int fp64, double* tflops) {
   return guarded([&] {

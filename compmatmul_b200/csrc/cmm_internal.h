@@ -10,6 +10,8 @@
 
 #include <cuda_runtime.h>
 
+#include "../../include/compmatmul_b200.h"
+
 namespace cmm {
 
 // ------------------------------------------------------------------ errors
@@ -115,6 +117,16 @@ void launch_hash_codes(int kind, const void* dHfns, const void* dSfns, int d, in
 void launch_hash_codes_keys(int kind, const void* dHfns, const void* dSfns, int d, int log2b,
                             int64_t n, const uint32_t* dKeys, uint32_t* dCodes, cudaStream_t s);
 
+// one code set of a batch: codes (d x n) of keys 0..n-1 under (H, S)
+struct HashJob {
+  const void* H;
+  const void* S;
+  uint32_t* codes;
+  int64_t n;
+  int d, log2b, kind;
+};
+void launch_hash_codes_jobs(const HashJob* dJobs, int njobs, int64_t max_total, cudaStream_t s);
+
 void launch_row_scale(const double* dAT, const double* dB, int64_t n_a, int64_t n_inner,
                       int64_t n_b, int* dScaleExp, cudaStream_t s);
 
@@ -204,6 +216,15 @@ void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const Sl
 void launch_finalize_natural(int variant, int d, int b, int G, const void* dPartial,
                              const double2* dTw, void* dWork, double* dP, cudaStream_t s);
 
+// Batched products (cmm_batch.cu); the product descriptor is the public
+// cmm_batch_product of compmatmul_b200.h.
+struct BatchPlan;
+BatchPlan* batch_create(const cmm_batch_product* products, int count, bool f32, bool tune);
+void batch_run(BatchPlan* B, cudaStream_t stream);
+void batch_info(const BatchPlan* B, int64_t* items, int* ctas, int* launches);
+void batch_config(const BatchPlan* B, int i, int* log2_slab, int* radix, int* groups, int* tuned);
+void batch_destroy(BatchPlan* B);
+
 // Top-K over a dense matrix; returns after synchronising s.
 void topk_dense(const double* dC, int64_t n_a, int64_t n_b, int K, uint32_t* dI, uint32_t* dJ,
                 double* dV, cudaStream_t s);
@@ -216,6 +237,7 @@ void prof_begin(const char* family, cudaStream_t s);
 void prof_end(const char* family, cudaStream_t s);
 void count_launch(int n = 1);
 void set_sketch_kernel(const char* name);  // recorded for cmm_last_sketch_kernel
+bool prof_set(bool on);                    // event profiling on/off; returns the previous state
 double probe_fma_tflops(bool fp64, cudaStream_t s);
 struct ProfScope {
   const char* fam;

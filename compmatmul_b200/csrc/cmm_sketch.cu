@@ -135,6 +135,37 @@ void launch_hash_codes(int kind, const void* dH, const void* dS, int d, int log2
   launch_hash_codes_keys(kind, dH, dS, d, log2b, n, nullptr, dCodes, s);
 }
 
+// Many independent code sets in one launch (batched products): block row y
+// serves job y; codes[t * n + i] for keys 0..n-1, t < d.
+__global__ void k_hash_codes_jobs(const HashJob* __restrict__ jobs) {
+  const HashJob J = jobs[blockIdx.y];
+  const int64_t total = J.n * (int64_t)J.d;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int t = (int)(e / J.n);
+    const uint32_t key = (uint32_t)(e - (int64_t)t * J.n);
+    uint32_t c;
+    switch (J.kind) {
+      case MS: c = hash_code<MS>(J.H, J.S, t, J.log2b, key); break;
+      case MAS: c = hash_code<MAS>(J.H, J.S, t, J.log2b, key); break;
+      case TAB8: c = hash_code<TAB8>(J.H, J.S, t, J.log2b, key); break;
+      default: c = hash_code<TAB16>(J.H, J.S, t, J.log2b, key); break;
+    }
+    J.codes[e] = c;
+  }
+}
+
+void launch_hash_codes_jobs(const HashJob* dJobs, int njobs, int64_t max_total, cudaStream_t s) {
+  if (njobs <= 0 || max_total <= 0) return;
+  const int threads = 256;
+  int64_t blocks = (max_total + threads - 1) / threads;
+  if (blocks > 1024) blocks = 1024;
+  ProfScope prof("hash", s);
+  count_launch();
+  k_hash_codes_jobs<<<dim3((unsigned)blocks, (unsigned)njobs), threads, 0, s>>>(dJobs);
+  CMM_CUDA(cudaGetLastError());
+}
+
 // --------------------------------------------------------------- row scale
 // e_k = round-to-zero((expo(max|AT[k,:]|) - expo(max|B[k,:]|)) / 2); the FFT
 // kernel scales the A row by 2^-e_k and the B row by 2^e_k (exact).

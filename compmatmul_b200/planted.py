@@ -75,3 +75,43 @@ def topk_dense_host(C, K):
     sel = cand[order][:K]
     n_b = C.shape[1]
     return sel // n_b, sel % n_b, flat[sel]
+
+
+def batch_shapes(count=256, seed=4004, lo=256, hi=4096):
+    """Shapes of the batched-products workload (config 4): m, n, p each
+    log-uniform in [lo, hi] (m = rows of C, n = inner, p = columns of C),
+    K = max(8, m // 64) planted entries, b = the next power of two >= 4 K 64,
+    d uniform in {5, 7, 9}, FFT or FWHT with probability 1/2 each."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        m, n, p = (int(round(float(np.exp(rng.uniform(np.log(lo), np.log(hi)))))) for _ in range(3))
+        K = max(8, m // 64)
+        K = min(K, m, n, p)
+        b = 1 << int(np.ceil(np.log2(4 * K * 64)))
+        d = int(rng.choice([5, 7, 9]))
+        variant = "fft" if rng.random() < 0.5 else "fwht"
+        out.append(dict(m=m, n=n, p=p, K=K, b=b, d=d, variant=variant, gen_seed=seed * 1000 + i,
+                        seed=seed + 17 * i))
+    return out
+
+
+def planted_problem_device(n_a, n_inner, n_b, K, gen_seed, dtype="float32", device="cuda",
+                           sigma=0.01, big=10.0):
+    """The planted generator of planted_problem with the noise drawn on the
+    device (torch generator seeded with gen_seed) and the planted triples
+    drawn on the host (numpy, gen_seed): returns (AT, B, (i, k, j))."""
+    import torch
+    dt = torch.float32 if dtype == "float32" else torch.float64
+    g = torch.Generator(device=device).manual_seed(int(gen_seed))
+    AT = torch.randn((n_inner, n_a), generator=g, device=device, dtype=dt) * sigma
+    B = torch.randn((n_inner, n_b), generator=g, device=device, dtype=dt) * sigma
+    rng = np.random.default_rng(gen_seed)
+    K = min(K, n_a, n_inner, n_b)
+    ks = rng.choice(n_inner, size=K, replace=False)
+    is_ = rng.choice(n_a, size=K, replace=False)
+    js = rng.choice(n_b, size=K, replace=False)
+    kt = torch.as_tensor(ks, device=device)
+    AT[kt, torch.as_tensor(is_, device=device)] += big
+    B[kt, torch.as_tensor(js, device=device)] += big
+    return AT, B, (is_, ks, js)

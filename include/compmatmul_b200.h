@@ -184,6 +184,54 @@ int cmm_matmul_f32(int variant, int hash_kind, int64_t n_a, int64_t n_inner, int
                    uint64_t seed);
 
 /* ---------------------------------------------------------------------
+ * Batched products (no reference twin: the reference computes one product
+ * per call).  A batch plan fixes a list of independent products of uneven
+ * shape -- each with its own variant, hash family, d, b, seed, sizes and
+ * device buffers -- and runs all of them per cmm_batch_run:
+ *   hash codes of every product (one launch), per-k row balance of the FFT
+ *   products (one launch), ONE persistent sketch launch whose CTAs pop work
+ *   items (product, repetition t, frequency slab, k-group) from a device
+ *   queue ordered longest first, then each product's k-group reduction +
+ *   inverse and (when C != NULL) dense median decompression.
+ * The whole sequence is captured in a CUDA graph on the first run and
+ * replayed afterwards.  Per product class (variant, precision, b, sizes) an
+ * autotuner times the candidate slab lengths and transform radices on the
+ * product's own data and caches the fastest (process-wide); the number of
+ * k-groups, hence CTAs per product, follows from the tuned per-row costs.
+ * Each product must have b <= 2^24; the device buffers must stay valid and
+ * unchanged in address for the plan's lifetime (their contents may change
+ * between runs).  Results equal cmm_dev_compressed_product /
+ * cmm_dev_matmul (FP64) or their _f32 forms on the same inputs, within
+ * the tolerances those state.
+ * ------------------------------------------------------------------- */
+typedef struct {
+  int variant;      /* CMM_VARIANT_FFT or CMM_VARIANT_FWHT */
+  int hash_kind;    /* cmm_hash_kind */
+  int d, b;
+  int64_t n_a, n_inner, n_b;
+  uint64_t seed;
+  const void* AT;   /* device, n_inner x n_a; float64, or float32 when the plan is f32 */
+  const void* B;    /* device, n_inner x n_b; same type */
+  double* p;        /* device, d x b sketch (output) */
+  double* C;        /* device, n_a x n_b dense estimate (output), or NULL for the sketch only */
+} cmm_batch_product;
+
+/* tune != 0 runs the autotuner for product classes not yet in its cache. */
+int cmm_batch_create(const cmm_batch_product* products, int count, int f32, int tune,
+                     void** handle);
+/* Runs every product of the plan on `stream` (NULL: an internal stream,
+ * synchronised before returning). */
+int cmm_batch_run(void* handle, void* stream);
+/* Work items of the persistent launch, its CTAs, and the kernel launches
+ * (graph kernel nodes) per run. */
+int cmm_batch_info(void* handle, int64_t* items, int* ctas, int* launches);
+/* The configuration chosen for one product: log2 of the slab length, the
+ * transform radix (4 or 8), the k-groups, and whether the autotuner timed it. */
+int cmm_batch_config(void* handle, int product, int* log2_slab, int* radix, int* groups,
+                     int* tuned);
+int cmm_batch_destroy(void* handle);
+
+/* ---------------------------------------------------------------------
  * Instrumentation for benchmarks (no reference twin).  When enabled, every
  * kernel launch of a family is bracketed by CUDA events recorded on the
  * stream it is launched on.  Families: "hash", "scale", "plan",
