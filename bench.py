@@ -49,6 +49,11 @@ def parse():
                     help="also time N steps of the plain FP64 path on the same inputs")
     ap.add_argument("--batch-count", type=int, default=256, help="products of the config4 batch")
     ap.add_argument("--batch-tune", type=int, default=1, help="config4: run the autotuner (0: defaults)")
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="config5: Poisson arrival rate (req/s)")
+    ap.add_argument("--serve-seconds", type=float, default=30.0, help="config5: arrival window (s)")
+    ap.add_argument("--serve-cap-gb", type=float, default=40.0, help="config5: admission cap (GB)")
+    ap.add_argument("--serve-streams", type=int, default=4, help="config5: waves in flight")
+    ap.add_argument("--serve-max-wave", type=int, default=64, help="config5: requests per wave")
     ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"],
                     help="fp64 = plain path; mixed = FP32 inputs (default for config3)")
     return ap.parse_args()
@@ -405,6 +410,128 @@ def bench_batch(args, world, rank, local):
         torch.distributed.destroy_process_group()
 
 
+# ------------------------------------------------------------ serving (config 5)
+def serve_stream(srv, pool, arrivals, poll_every=64):
+    """Submits pool[i % len(pool)] at arrivals[i] (seconds from start) and
+    collects completions as they come; returns (latencies, span_s)."""
+    from collections import deque
+    out = deque()
+    lat = []
+    t0 = time.perf_counter()
+    for i, ta in enumerate(arrivals):
+        while True:
+            dt = ta - (time.perf_counter() - t0)
+            if dt <= 0:
+                break
+            if dt > 0.002:
+                time.sleep(dt - 0.001)
+        q = pool[i % len(pool)]
+        out.append(srv.submit(q["AT"], q["B"], q["d"], q["b"], q["seed"], q["variant"]))
+        if i % poll_every == 0:
+            while out:
+                done, l = srv.wait(out[0], 0.0)
+                if not done:
+                    break
+                lat.append(l)
+                srv._live.pop(out.popleft(), None)
+    while out:
+        rid = out.popleft()
+        done, l = srv.wait(rid, None)
+        lat.append(l)
+        srv._live.pop(rid, None)
+    span = time.perf_counter() - t0
+    return np.array(lat), span
+
+
+def bench_serve(args, world, rank, local):
+    """Config 5: Poisson arrivals (rate, duration) of requests sized as the
+    batched config, served with continuous batching under a device-memory
+    admission cap; latency p50/p99 and products/s, against the plain FP64
+    path on the same stream."""
+    import torch
+    import compmatmul_b200 as cmb
+    from compmatmul_b200.batch import BatchPlan
+    from compmatmul_b200.planted import batch_shapes, planted_problem_device
+    from compmatmul_b200.serve import Server
+    rate, secs, cap = args.serve_rate, args.serve_seconds, int(args.serve_cap_gb * (1 << 30))
+    config = {"workload": f"config5: Poisson arrivals at {rate:g} req/s for {secs:g} s; each request one compressed "
+                          f"product sized as config4 (m, n, p log-uniform in [256, 4096], FP32, planted, "
+                          f"b = next pow2 >= 256 K, d in {{5,7,9}}, FFT/FWHT 50/50) from a pool of "
+                          f"{args.batch_count} inputs; admission cap {args.serve_cap_gb:g} GB; result = sketch p",
+              "rate_per_s": rate, "seconds": secs, "cap_bytes": cap}
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving loop; its per-product "
+                              "CPU cost is the config4 reference line"}), flush=True)
+        return
+    torch.cuda.set_device(local if world > 1 else 0)
+    shapes = batch_shapes(count=args.batch_count, seed=5005 + 1000 * rank)
+    pool = []
+    for sh in shapes:
+        AT, B, _ = planted_problem_device(sh["m"], sh["n"], sh["p"], sh["K"], sh["gen_seed"], "float32")
+        pool.append(dict(AT=AT, B=B, d=sh["d"], b=sh["b"], seed=sh["seed"], variant=sh["variant"]))
+    # the autotuner's cache covers the request classes before the stream starts
+    BatchPlan(pool, f32=True, tune=True, dense=False).close()
+    rng = np.random.default_rng(77 + rank)
+    n_req = int(rate * secs)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
+    L = cmb.lib()
+
+    def run(pool_, f32, arr, streams=args.serve_streams):
+        srv = Server(mem_cap_bytes=cap, f32=f32, streams=streams, max_wave=args.serve_max_wave)
+        warm = [srv.submit(q["AT"], q["B"], q["d"], q["b"], q["seed"], q["variant"]) for q in pool_[:8]]
+        for w in warm:
+            srv.result(w)
+        l0 = L.cmm_launch_count()
+        clocks = ClockSampler(torch.cuda.current_device())
+        clocks.start()
+        lat, span = serve_stream(srv, pool_, arr)
+        clk = clocks.stop()
+        st = srv.stats()
+        srv.close()
+        return {"products_per_s": len(lat) / span, "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                "p99_ms": float(np.percentile(lat, 99) * 1e3), "mean_ms": float(lat.mean() * 1e3),
+                "requests": int(len(lat)), "span_s": span, "waves": int(st["waves"] - 1),
+                "max_waves_in_flight": int(st["max_waves_in_flight"]),
+                "max_mem_in_use_bytes": int(st["max_mem_in_use"]), "launches": int(L.cmm_launch_count() - l0),
+                "clocks": clk}
+
+    main_run = run(pool, True, arrivals)
+    # latency without queueing: half the measured capacity, 10 s
+    light_rate = 0.5 * main_run["products_per_s"]
+    light = run(pool, True, np.cumsum(rng.exponential(1.0 / light_rate, size=int(light_rate * 10))))
+    light["rate_per_s"] = light_rate
+    # host payloads (pinned), H2D inside each request
+    hpool = [dict(q, AT=q["AT"].cpu().pin_memory(), B=q["B"].cpu().pin_memory()) for q in pool[:64]]
+    host = run(hpool, True, np.cumsum(rng.exponential(1.0 / light_rate, size=int(light_rate * 10))))
+    host["rate_per_s"] = light_rate
+    h2d = float(np.mean([q["AT"].numel() * 4 + q["B"].numel() * 4 for q in hpool]))
+    d2h = float(np.mean([q["d"] * q["b"] * 8 for q in hpool]))
+    del hpool
+    fp64 = None
+    if args.compare_fp64:
+        pool64 = [dict(q, AT=q["AT"].double(), B=q["B"].double()) for q in pool]
+        fp64 = run(pool64, False, arrivals)
+        del pool64
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": main_run["products_per_s"], "unit": "products/s", "n_gpus": world,
+        "steps": main_run["requests"], "warmup": 8, "ms_per_step": 1e3 / main_run["products_per_s"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (mixed: FP32 transforms, FP64 reduction)", "data": "synthetic", "config": config,
+        "latency_ms": {"p50": main_run["p50_ms"], "p99": main_run["p99_ms"], "mean": main_run["mean_ms"]},
+        "serving": main_run, "unsaturated": light, "host_payload": host,
+        "e2e": {"value": host["products_per_s"], "unit": "products/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": main_run["launches"], "clocks": main_run["clocks"], "roofline": None, "cpu_baseline": None,
+    }
+    if fp64 is not None:
+        line["plain_fp64_same_stream"] = fp64
+        line["plain_fp64_same_stream"]["speedup"] = main_run["products_per_s"] / fp64["products_per_s"]
+    print(json.dumps(line), flush=True)
+
+
 # --------------------------------------------------------------- main
 def main():
     args = parse()
@@ -413,6 +540,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.workload == "config4":
         bench_batch(args, world, rank, local)
+        return
+    if args.workload == "config5":
+        bench_serve(args, world, rank, local)
         return
     from compmatmul_b200.planted import WORKLOADS, planted_problem
     w = dict(WORKLOADS[args.workload])

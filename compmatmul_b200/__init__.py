@@ -37,7 +37,8 @@ EXPORTED = [
     "cmm_launch_count", "cmm_dev_compressed_product_f32", "cmm_dev_matmul_f32",
     "cmm_compressed_product_f32", "cmm_matmul_f32", "cmm_dev_compressed_product_noalloc",
     "cmm_last_sketch_kernel", "cmm_probe_fma_tflops", "cmm_batch_create", "cmm_batch_run",
-    "cmm_batch_info", "cmm_batch_config", "cmm_batch_destroy",
+    "cmm_batch_info", "cmm_batch_config", "cmm_batch_destroy", "cmm_server_create", "cmm_server_submit",
+    "cmm_server_wait", "cmm_server_stats_get", "cmm_server_destroy",
 ]
 
 
@@ -72,6 +73,11 @@ def lib():
     L.cmm_batch_config.argtypes = [vp, i32, _C.POINTER(_C.c_int), _C.POINTER(_C.c_int),
                                    _C.POINTER(_C.c_int), _C.POINTER(_C.c_int)]
     L.cmm_batch_destroy.argtypes = [vp]
+    L.cmm_server_create.argtypes = [vp, _C.POINTER(_C.c_void_p)]
+    L.cmm_server_submit.argtypes = [vp, vp, _C.POINTER(_C.c_uint64)]
+    L.cmm_server_wait.argtypes = [vp, u64, _C.c_double, _C.POINTER(_C.c_int), _C.POINTER(_C.c_double)]
+    L.cmm_server_stats_get.argtypes = [vp, vp]
+    L.cmm_server_destroy.argtypes = [vp]
     L.cmm_device_count.restype = i32
     L.cmm_max_buckets.restype = i32
     L.cmm_matmul.argtypes = [i32, i32, i64, i64, i64, dp, dp, dp, i32, i32, i32, u64]

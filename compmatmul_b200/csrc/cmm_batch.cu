@@ -31,14 +31,14 @@
 #include <vector>
 
 #include "../../include/compmatmul_b200.h"
-#include "cmm_internal.h"
+#include "cmm_batch.h"
 
 namespace cmm {
 namespace {
 
 constexpr int kBT = 1024;        // threads per CTA
-constexpr int kBFftLog = 12;     // largest FFT slab (complex)
-constexpr int kBWhtLog = 13;     // largest FWHT slab (real, x and y)
+constexpr int kBFftLog = kBatchFftLog;
+constexpr int kBWhtLog = kBatchWhtLog;
 constexpr int kBSkip = -0x7fffffff;
 
 // ------------------------------------------------------------- helpers
@@ -218,31 +218,6 @@ __device__ __forceinline__ void h16_stage(float* buf, int L, int sh, const uint3
 }
 
 }  // namespace
-
-// device-side description of one product of a batch
-struct BProd {
-  const void* AT;
-  const void* B;
-  // per repetition t, the indices of each side stably sorted by slab
-  // position h mod L (t-major, SA / SB slots per t): source index | (sign ==
-  // +1) << 31, the bucket h itself (u16 when code16), and kPlanThreads + 1
-  // cut offsets that split the slots into per-thread runs of whole buckets
-  const uint32_t* srcA;
-  const uint32_t* srcB;
-  const void* codeA;
-  const void* codeB;
-  const uint32_t* cutA;
-  const uint32_t* cutB;
-  const int* scale;        // FFT row exponents, n_inner
-  const double2* tw;       // w_b^j, j < b
-  void* partial;           // [G][d][R][L] (double2 FFT, double FWHT)
-  int64_t n_a, n_inner, n_b;
-  int SA, SB, code16;
-  int d, log2b, logL, logR, G, variant, radix;
-};
-struct BItem {
-  int prod, t, r, g;
-};
 
 template <typename Real>
 __global__ void __launch_bounds__(kBT, 1)
@@ -588,6 +563,29 @@ int resident_ctas() {
 }
 
 }  // namespace
+
+int batch_resident_ctas(bool f32) { return f32 ? resident_ctas<float>() : resident_ctas<double>(); }
+
+void batch_launch_sketch(bool f32, const BProd* dP, const BItem* dI, int n_items, int* dCounter,
+                         const double2* tw4096, int ctas, cudaStream_t s) {
+  if (n_items <= 0) return;
+  if (f32) launch_sketch<float>(dP, dI, n_items, dCounter, tw4096, ctas, s);
+  else launch_sketch<double>(dP, dI, n_items, dCounter, tw4096, ctas, s);
+}
+
+bool batch_tuned(int variant, bool f32, int log2b, int64_t n_ab, int* logL, int* radix) {
+  const TuneKey key{variant, (int)f32, log2b, ilog2c(std::max<int64_t>(n_ab, 1))};
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  auto it = g_tune.find(key);
+  if (it == g_tune.end()) return false;
+  *logL = it->second.logL;
+  *radix = it->second.radix;
+  return true;
+}
+
+double batch_unit_cost(int64_t n_a, int64_t n_b, int logL) {
+  return 4.0 * (double)(n_a + n_b) + (double)(1 << logL) * (double)std::max(logL, 1);
+}
 
 struct BatchPlan {
   bool f32 = false;

@@ -493,6 +493,36 @@ int cmm_batch_destroy(void* handle) {
   return guarded([&] { batch_destroy(static_cast<BatchPlan*>(handle)); });
 }
 
+int cmm_server_create(const cmm_server_config* cfg, void** server) {
+  return guarded([&] {
+    if (!server) throw invalid_argument("server must not be null");
+    *server = nullptr;
+    *server = server_create(cfg);
+  });
+}
+
+int cmm_server_submit(void* server, const cmm_request* req, uint64_t* id) {
+  return guarded([&] {
+    const uint64_t v = server_submit(static_cast<Server*>(server), req);
+    if (id) *id = v;
+  });
+}
+
+int cmm_server_wait(void* server, uint64_t id, double timeout_s, int* done, double* latency_s) {
+  return guarded([&] {
+    const bool d = server_wait(static_cast<Server*>(server), id, timeout_s, latency_s);
+    if (done) *done = d ? 1 : 0;
+  });
+}
+
+int cmm_server_stats_get(void* server, cmm_server_stats* out) {
+  return guarded([&] { server_stats(static_cast<Server*>(server), out); });
+}
+
+int cmm_server_destroy(void* server) {
+  return guarded([&] { server_destroy(static_cast<Server*>(server)); });
+}
+
 int cmm_probe_fma_tflops(int fp64, double* tflops) {
   return guarded([&] {
     if (!tflops) throw invalid_argument("tflops must not be null");

@@ -225,6 +225,14 @@ void batch_info(const BatchPlan* B, int64_t* items, int* ctas, int* launches);
 void batch_config(const BatchPlan* B, int i, int* log2_slab, int* radix, int* groups, int* tuned);
 void batch_destroy(BatchPlan* B);
 
+// Serving engine (cmm_serve.cu)
+struct Server;
+Server* server_create(const cmm_server_config* cfg);
+uint64_t server_submit(Server* S, const cmm_request* req);
+bool server_wait(Server* S, uint64_t id, double timeout_s, double* latency_s);
+void server_stats(Server* S, cmm_server_stats* out);
+void server_destroy(Server* S);
+
 // Top-K over a dense matrix; returns after synchronising s.
 void topk_dense(const double* dC, int64_t n_a, int64_t n_b, int K, uint32_t* dI, uint32_t* dJ,
                 double* dV, cudaStream_t s);

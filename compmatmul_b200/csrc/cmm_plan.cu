@@ -422,16 +422,22 @@ SlabPlan make_residue_plan(const uint32_t* dCodesA, const uint32_t* dCodesB, int
         cut.as<uint32_t>(), emax.as<uint32_t>());
     CMM_CUDA(cudaGetLastError());
   }
-  std::vector<uint32_t> h((size_t)d * 2 * R2);
-  CMM_CUDA(cudaMemcpyAsync(h.data(), emax.ptr, h.size() * 4, cudaMemcpyDeviceToHost, s));
-  CMM_CUDA(cudaStreamSynchronize(s));
-  // compact segments: S = the largest segment (over t and r2), rounded to 8
+  // compact segments: S = the largest segment (over t and r2), rounded to 8;
+  // with one segment (R2 = 1) it holds every index, so no read-back is needed
   uint32_t SA = 8, SB = 8;
-  for (int t = 0; t < d; ++t)
-    for (int r = 0; r < R2; ++r) {
-      SA = h[((size_t)t * 2 + 0) * R2 + r] > SA ? h[((size_t)t * 2 + 0) * R2 + r] : SA;
-      SB = h[((size_t)t * 2 + 1) * R2 + r] > SB ? h[((size_t)t * 2 + 1) * R2 + r] : SB;
-    }
+  if (R2 == 1) {
+    SA = n_a > 8 ? (uint32_t)n_a : 8u;
+    SB = n_b > 8 ? (uint32_t)n_b : 8u;
+  } else {
+    std::vector<uint32_t> h((size_t)d * 2 * R2);
+    CMM_CUDA(cudaMemcpyAsync(h.data(), emax.ptr, h.size() * 4, cudaMemcpyDeviceToHost, s));
+    CMM_CUDA(cudaStreamSynchronize(s));
+    for (int t = 0; t < d; ++t)
+      for (int r = 0; r < R2; ++r) {
+        SA = h[((size_t)t * 2 + 0) * R2 + r] > SA ? h[((size_t)t * 2 + 0) * R2 + r] : SA;
+        SB = h[((size_t)t * 2 + 1) * R2 + r] > SB ? h[((size_t)t * 2 + 1) * R2 + r] : SB;
+      }
+  }
   SA = (SA + 7) & ~7u;
   SB = (SB + 7) & ~7u;
   P.compact = true;

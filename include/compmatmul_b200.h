@@ -232,6 +232,56 @@ int cmm_batch_config(void* handle, int product, int* log2_slab, int* radix, int*
 int cmm_batch_destroy(void* handle);
 
 /* ---------------------------------------------------------------------
+ * Serving (no reference twin): continuous batching of independent
+ * compressed products.  A background scheduler admits submitted requests in
+ * arrival order while the device memory they hold stays under the cap
+ * (inputs when copied in, hash codes, sorted plans, row balance, k-group
+ * partials, the sketch), prepares each on an upload stream, groups the
+ * prepared ones into waves -- each wave is one persistent sketch launch over
+ * all of its products' work items plus their reduction + inverse -- and runs
+ * waves on several streams at once, so requests that arrive while others
+ * run are admitted as memory frees up and their work overlaps on the device.
+ * The sketch p of each request is copied back to the caller's host buffer.
+ * A request's result does not depend on what it was batched with: its work
+ * items and their order are fixed by the request alone.
+ * ------------------------------------------------------------------- */
+typedef struct {
+  size_t mem_cap_bytes;  /* admission cap on device bytes held by admitted requests */
+  int f32;               /* 1: float32 inputs (mixed precision); 0: float64 */
+  int streams;           /* waves in flight at once (>= 1) */
+  int max_wave;          /* most requests per wave (>= 1) */
+} cmm_server_config;
+
+typedef struct {
+  int variant, hash_kind, d, b;
+  int64_t n_a, n_inner, n_b;
+  uint64_t seed;
+  const void* AT;      /* n_inner x n_a, float32 or float64 per the server */
+  const void* B;       /* n_inner x n_b */
+  int inputs_on_device; /* 1: AT, B are device pointers; 0: host (pinned host memory copies asynchronously) */
+  double* p;           /* host d x b output */
+} cmm_request;
+
+typedef struct {
+  int64_t submitted, completed, queued, in_flight;
+  int64_t waves, max_waves_in_flight;
+  size_t mem_in_use, max_mem_in_use;
+} cmm_server_stats;
+
+int cmm_server_create(const cmm_server_config* cfg, void** server);
+/* Queues one request (its buffers must stay valid until it completes);
+ * *id identifies it.  A request that alone needs more than the cap is
+ * rejected with CMM_ERR_INVALID_ARGUMENT. */
+int cmm_server_submit(void* server, const cmm_request* req, uint64_t* id);
+/* Waits up to timeout_s seconds (< 0: no limit) for request id; *done = 1
+ * when its p is in the host buffer.  *latency_s (may be NULL) = submit to
+ * completion, seconds. */
+int cmm_server_wait(void* server, uint64_t id, double timeout_s, int* done, double* latency_s);
+int cmm_server_stats_get(void* server, cmm_server_stats* out);
+/* Drains every queued request, then stops the scheduler and frees all. */
+int cmm_server_destroy(void* server);
+
+/* ---------------------------------------------------------------------
  * Instrumentation for benchmarks (no reference twin).  When enabled, every
  * kernel launch of a family is bracketed by CUDA events recorded on the
  * stream it is launched on.  Families: "hash", "scale", "plan",

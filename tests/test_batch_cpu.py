@@ -46,3 +46,11 @@ def test_batch_null_handle_calls():
     assert L.cmm_batch_run(None, None) == 1
     assert "null" in L.cmm_last_error().decode()
     assert L.cmm_batch_destroy(None) == 0
+
+
+def test_server_null_handle_calls():
+    L = lib()
+    rid = C.c_uint64()
+    assert L.cmm_server_submit(None, None, C.byref(rid)) == 1
+    assert "null" in L.cmm_last_error().decode()
+    assert L.cmm_server_destroy(None) == 0
