@@ -83,6 +83,39 @@ __device__ __forceinline__ void r8(C (&x)[8], C W) {
   const C W3 = cmul(W, mk(-h, -h));
   bf(x[0], x[4], W); bf(x[1], x[5], W1); bf(x[2], x[6], Wi); bf(x[3], x[7], W3);
 }
+// the same steps for kk = 0 (W = 1): the twiddles are 1, -i and w_8^{1,3}
+template <typename C>
+__device__ __forceinline__ void add_sub(C& a, C& b) {
+  const C t = b;
+  b = mk(a.x - t.x, a.y - t.y);
+  a = mk(a.x + t.x, a.y + t.y);
+}
+template <typename C>
+__device__ __forceinline__ C mul_mi(C a) { return mk(a.y, -a.x); }  // a * (-i)
+template <typename C>
+__device__ __forceinline__ void r4_first(C (&x)[4]) {
+  add_sub(x[0], x[1]);
+  add_sub(x[2], x[3]);
+  add_sub(x[0], x[2]);
+  x[3] = mul_mi(x[3]);
+  add_sub(x[1], x[3]);
+}
+template <typename C>
+__device__ __forceinline__ void r8_first(C (&x)[8]) {
+  using R = decltype(x[0].x);
+  const R h = (R)0.70710678118654752440;
+  add_sub(x[0], x[1]); add_sub(x[2], x[3]); add_sub(x[4], x[5]); add_sub(x[6], x[7]);
+  add_sub(x[0], x[2]); add_sub(x[4], x[6]);
+  x[3] = mul_mi(x[3]); x[7] = mul_mi(x[7]);
+  add_sub(x[1], x[3]); add_sub(x[5], x[7]);
+  add_sub(x[0], x[4]);
+  x[5] = mk((x[5].x + x[5].y) * h, (x[5].y - x[5].x) * h);    // * w_8
+  add_sub(x[1], x[5]);
+  x[6] = mul_mi(x[6]);
+  add_sub(x[2], x[6]);
+  x[7] = mk((x[7].y - x[7].x) * h, -(x[7].x + x[7].y) * h);   // * w_8^3
+  add_sub(x[3], x[7]);
+}
 template <typename R, int M>
 __device__ __forceinline__ void whtr(R (&x)[M]) {
 #pragma unroll
@@ -114,32 +147,37 @@ __host__ __device__ constexpr int ph_len(int L) {
   return ES == 16 ? L + L / 8 : (ES == 8 ? L + L / 16 : L + L / 32);
 }
 
-// one DIT pass of radix K over L points (bit-reversed in); the pass twiddle
-// w_4096^j comes from two 64-entry tables: wh[j >> 6] * wl[j & 63]
-template <int K, typename C>
-__device__ __forceinline__ void fft_pass(C* buf, int L, int s, const C* wh, const C* wl, const C* add, int ti,
-                                         int nt) {
+// one DIT pass of radix K over L points (bit-reversed in); wt[j] = w_4096^j.
+// The first pass (s = 0, all twiddles trivial) adds side B's sub-sequence on
+// load and clears it for the next row.
+template <int K, bool FIRST, typename C>
+__device__ __forceinline__ void fft_pass(C* buf, C* add, int L, int s, const C* wt, int ti, int nt) {
   constexpr int ES = (int)sizeof(C);
   constexpr int LK = K == 8 ? 3 : (K == 4 ? 2 : 1);
   const int half = 1 << s;
   for (int p = ti; p < (L >> LK); p += nt) {
     const int kk = p & (half - 1);
     const int base = ((p >> s) << (s + LK)) | kk;
-    const int j = kk << (kBFftLog - s - LK);
-    const C W = cmul(wh[j >> 6], wl[j & 63]);  // w_{K half}^kk
     C x[K];
 #pragma unroll
     for (int e = 0; e < K; ++e) x[e] = buf[ph<ES>(base + e * half)];
-    if (add) {  // first pass: the two sides' sub-sequences are summed on load
+    if constexpr (FIRST) {
 #pragma unroll
       for (int e = 0; e < K; ++e) {
-        const C y = add[ph<ES>(base + e * half)];
+        C* q = add + ph<ES>(base + e * half);
+        const C y = *q;
+        *q = mk(decltype(y.x)(0), decltype(y.x)(0));
         x[e] = mk(x[e].x + y.x, x[e].y + y.y);
       }
+      if constexpr (K == 8) r8_first(x);
+      else if constexpr (K == 4) r4_first(x);
+      else add_sub(x[0], x[1]);
+    } else {
+      const C W = wt[kk << (kBFftLog - s - LK)];  // w_{K half}^kk
+      if constexpr (K == 8) r8(x, W);
+      else if constexpr (K == 4) r4(x, W);
+      else bf(x[0], x[1], W);
     }
-    if constexpr (K == 8) r8(x, W);
-    else if constexpr (K == 4) r4(x, W);
-    else bf(x[0], x[1], W);
 #pragma unroll
     for (int e = 0; e < K; ++e) buf[ph<ES>(base + e * half)] = x[e];
   }
@@ -236,9 +274,8 @@ __global__ void __launch_bounds__(kBT, 1)
   extern __shared__ __align__(16) unsigned char sm[];
   const int tid = threadIdx.x, lane = tid & 31;
   const int q = tid / NT, ti = tid % NT;  // this thread's row slot and its index within it
-  C* wh = reinterpret_cast<C*>(sm + KB * kSeq);  // w_4096^{64 a}, a < 64
-  C* wl = wh + 64;                               // w_4096^c, c < 64
-  C* dh = wl + 64;                               // DIF weights w_b^x = dh[x >> sd] * dl[x & (2^sd - 1)]
+  C* wt = reinterpret_cast<C*>(sm + KB * kSeq);  // pass twiddles w_4096^j, j < 4096
+  C* dh = wt + (1 << kBFftLog);                  // DIF weights w_b^x = dh[x >> sd] * dl[x & (2^sd - 1)]
   C* dl = dh + 256;                              //   (b <= 2^16; larger b reads the global table)
   // row slot qq: FFT sides A, B (A also holds the transform); FWHT x, y
   auto bufA = [&](int qq) { return reinterpret_cast<C*>(sm + qq * kSeq); };
@@ -246,10 +283,11 @@ __global__ void __launch_bounds__(kBT, 1)
   auto xsq = [&](int qq) { return reinterpret_cast<Real*>(sm + qq * kSeq); };
   auto ysq = [&](int qq) { return reinterpret_cast<Real*>(sm + qq * kSeq) + PLW; };
   __shared__ int s_item, s_log2b;
-  for (int j = tid; j < 64; j += kBT) {
-    wh[j] = mk((Real)tw4096[j << 6].x, (Real)tw4096[j << 6].y);
-    wl[j] = mk((Real)tw4096[j].x, (Real)tw4096[j].y);
-  }
+  for (int j = tid; j < (1 << kBFftLog); j += kBT) wt[j] = mk((Real)tw4096[j].x, (Real)tw4096[j].y);
+  // every row slot starts clear; the passes and the accumulation clear what
+  // they consume, so the slots are clear again before each row's scatter
+  for (size_t e = tid * 16; e < KB * kSeq; e += kBT * 16)
+    *reinterpret_cast<uint4*>(sm + e) = make_uint4(0u, 0u, 0u, 0u);
   if (tid == 0) s_log2b = -1;
   uint32_t hb[2][2] = {{0u, 0u}, {0u, 0u}};
   if (kF32) {
@@ -306,16 +344,6 @@ __global__ void __launch_bounds__(kBT, 1)
         se = __ldg(P.scale + k);
         live = se != kBSkip;  // a zero row: the slot stays zero and adds nothing
       }
-      if (fft) {
-        C* A = bufA(q);
-        C* Bq = bufB(q);
-        for (int e = ti; e < ph_len<EC>(L); e += NT) { A[e] = mk((Real)0, (Real)0); Bq[e] = mk((Real)0, (Real)0); }
-      } else {
-        Real* xs = xsq(q);
-        Real* ys = ysq(q);
-        for (int e = ti; e < ph_len<ER>(L); e += NT) { xs[e] = (Real)0; ys[e] = (Real)0; }
-      }
-      __syncthreads();
       // ---- count sketch + DIF split: one store per bucket (no atomics)
       if (live) {
         for (int side = side0; side <= side1; ++side) {
@@ -386,12 +414,16 @@ __global__ void __launch_bounds__(kBT, 1)
       // ---- transform of this thread's row slot
       if (fft) {
         C* A = bufA(q);
-        const C* Bq = bufB(q);
+        C* Bq = bufB(q);
         int s = 0;
+        if (P.radix == 8 && logL >= 3) fft_pass<8, true>(A, Bq, L, 0, wt, ti, NT), s = 3;
+        else if (logL >= 2) fft_pass<4, true>(A, Bq, L, 0, wt, ti, NT), s = 2;
+        else fft_pass<2, true>(A, Bq, L, 0, wt, ti, NT), s = 1;
+        __syncthreads();
         if (P.radix == 8)
-          for (; s + 3 <= logL; s += 3) { fft_pass<8>(A, L, s, wh, wl, s == 0 ? Bq : nullptr, ti, NT); __syncthreads(); }
-        for (; s + 2 <= logL; s += 2) { fft_pass<4>(A, L, s, wh, wl, s == 0 ? Bq : nullptr, ti, NT); __syncthreads(); }
-        if (s < logL) { fft_pass<2>(A, L, s, wh, wl, s == 0 ? Bq : nullptr, ti, NT); __syncthreads(); }
+          for (; s + 3 <= logL; s += 3) { fft_pass<8, false>(A, Bq, L, s, wt, ti, NT); __syncthreads(); }
+        for (; s + 2 <= logL; s += 2) { fft_pass<4, false>(A, Bq, L, s, wt, ti, NT); __syncthreads(); }
+        if (s < logL) { fft_pass<2, false>(A, Bq, L, s, wt, ti, NT); __syncthreads(); }
       } else {
         Real* xs = xsq(q);
         Real* ys = ysq(q);
@@ -418,7 +450,9 @@ __global__ void __launch_bounds__(kBT, 1)
           if (m < L) {
 #pragma unroll
             for (int qq = 0; qq < KB; ++qq) {
-              const C z = bufA(qq)[ph<EC>(m)];
+              C* zp = bufA(qq) + ph<EC>(m);
+              const C z = *zp;
+              *zp = mk((Real)0, (Real)0);  // clear for the next row
               if constexpr (kF32) {
                 tsum(acc[2 * j], lo[2 * j], z.x * z.x - z.y * z.y);
                 tsum(acc[2 * j + 1], lo[2 * j + 1], (z.x + z.x) * z.y);
@@ -436,9 +470,13 @@ __global__ void __launch_bounds__(kBT, 1)
           if (m < L) {
 #pragma unroll
             for (int qq = 0; qq < KB; ++qq) {
-              const Real pxy = xsq(qq)[ph<ER>(m)] * ysq(qq)[ph<ER>(m)];
-              if constexpr (kF32) tsum(acc[j], lo[j], pxy);
-              else acc[j] = fma(xsq(qq)[ph<ER>(m)], ysq(qq)[ph<ER>(m)], acc[j]);
+              Real* xp = xsq(qq) + ph<ER>(m);
+              Real* yp = ysq(qq) + ph<ER>(m);
+              const Real xv = *xp, yv = *yp;
+              *xp = (Real)0;  // clear for the next row
+              *yp = (Real)0;
+              if constexpr (kF32) tsum(acc[j], lo[j], xv * yv);
+              else acc[j] = fma(xv, yv, acc[j]);
             }
           }
         }
@@ -536,7 +574,7 @@ size_t smem_bytes(bool f32) {
   const size_t L = (size_t)1 << kBFftLog, W = (size_t)1 << kBWhtLog;
   const size_t plf = f32 ? L + L / 16 : L + L / 8, plw = f32 ? W + W / 32 : W + W / 16;
   const size_t per_row = std::max(2 * plf * cpx, 2 * plw * real);
-  return (f32 ? 2 : 1) * per_row + (64 + 64 + 256 + 256) * cpx;
+  return (f32 ? 2 : 1) * per_row + (L + 256 + 256) * cpx;
 }
 
 template <typename Real>
