@@ -49,6 +49,8 @@ def parse():
                     help="also time N steps of the plain FP64 path on the same inputs")
     ap.add_argument("--batch-count", type=int, default=256, help="products of the config4 batch")
     ap.add_argument("--batch-tune", type=int, default=1, help="config4: run the autotuner (0: defaults)")
+    ap.add_argument("--batch-variant", default="both", choices=["both", "fft", "fwht"],
+                    help="config4: draw the variants as specified (both) or force one")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="config5: Poisson arrival rate (req/s)")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="config5: arrival window (s)")
     ap.add_argument("--serve-cap-gb", type=float, default=40.0, help="config5: admission cap (GB)")
@@ -189,6 +191,8 @@ def bench_batch(args, world, rank, local):
     from compmatmul_b200.planted import batch_shapes, planted_problem_device
     count = args.batch_count
     shapes = batch_shapes(count=count, seed=4004 + 1000 * rank)
+    if args.batch_variant != "both":  # one variant only (component timing)
+        shapes = [dict(s, variant=args.batch_variant) for s in shapes]
     config = {"workload": f"config4: {count} planted products m x n x p, each dimension log-uniform in "
                           f"[256, 4096], FP32 noise N(0,0.01^2) + K=max(8,m/64) planted +10/+10, "
                           f"b = next pow2 >= 256 K, d in {{5,7,9}}, FFT/FWHT 50/50; sketch + dense median "

@@ -182,6 +182,74 @@ __device__ __forceinline__ void fft_pass(C* buf, C* add, int L, int s, const C* 
     for (int e = 0; e < K; ++e) buf[ph<ES>(base + e * half)] = x[e];
   }
 }
+// padded address of x + e * half for the compile-time stride HALF: linear
+// in e once HALF is a multiple of the padding period
+template <int ES, int HALF>
+__device__ __forceinline__ int ph_step(int base, int e) {
+  constexpr int P = ES == 16 ? 8 : (ES == 8 ? 16 : 32);  // elements per padding slot
+  if constexpr (HALF % P == 0) return ph<ES>(base) + e * (HALF + HALF / P);
+  else return ph<ES>(base + e * HALF);
+}
+
+// fft_pass with the slab length, stage and thread count fixed at compile
+// time (the common slabs): every index is a constant offset from one base
+template <int K, bool FIRST, int LOGL, int S, int NT, typename C>
+__device__ __forceinline__ void fft_pass_fixed(C* buf, C* add, const C* wt, int ti) {
+  constexpr int ES = (int)sizeof(C);
+  constexpr int LK = K == 8 ? 3 : (K == 4 ? 2 : 1);
+  constexpr int HALF = 1 << S;
+  constexpr int GROUPS = (1 << LOGL) >> LK;
+#pragma unroll
+  for (int p0 = 0; p0 < GROUPS; p0 += NT) {
+    const int p = p0 + ti;
+    if (GROUPS % NT != 0 && p >= GROUPS) break;
+    const int kk = p & (HALF - 1);
+    const int base = ((p >> S) << (S + LK)) | kk;
+    C x[K];
+#pragma unroll
+    for (int e = 0; e < K; ++e) x[e] = buf[ph_step<ES, HALF>(base, e)];
+    if constexpr (FIRST) {
+#pragma unroll
+      for (int e = 0; e < K; ++e) {
+        C* q = add + ph_step<ES, HALF>(base, e);
+        const C y = *q;
+        *q = mk(decltype(y.x)(0), decltype(y.x)(0));
+        x[e] = mk(x[e].x + y.x, x[e].y + y.y);
+      }
+      if constexpr (K == 8) r8_first(x);
+      else if constexpr (K == 4) r4_first(x);
+      else add_sub(x[0], x[1]);
+    } else {
+      const C W = wt[kk << (kBFftLog - S - LK)];
+      if constexpr (K == 8) r8(x, W);
+      else if constexpr (K == 4) r4(x, W);
+      else bf(x[0], x[1], W);
+    }
+#pragma unroll
+    for (int e = 0; e < K; ++e) buf[ph_step<ES, HALF>(base, e)] = x[e];
+  }
+}
+
+template <int K, int LOGL, int S, int NT, typename R>
+__device__ __forceinline__ void wht_pass_fixed(R* arr, int ti) {
+  constexpr int ES = (int)sizeof(R);
+  constexpr int LK = K == 8 ? 3 : (K == 4 ? 2 : 1);
+  constexpr int HALF = 1 << S;
+  constexpr int GROUPS = (1 << LOGL) >> LK;
+#pragma unroll
+  for (int p0 = 0; p0 < GROUPS; p0 += NT) {
+    const int p = p0 + ti;
+    if (GROUPS % NT != 0 && p >= GROUPS) break;
+    const int base = ((p >> S) << (S + LK)) | (p & (HALF - 1));
+    R x[K];
+#pragma unroll
+    for (int e = 0; e < K; ++e) x[e] = arr[ph_step<ES, HALF>(base, e)];
+    whtr<R, K>(x);
+#pragma unroll
+    for (int e = 0; e < K; ++e) arr[ph_step<ES, HALF>(base, e)] = x[e];
+  }
+}
+
 // one natural-order WHT pass of radix K over L points
 template <int K, typename R>
 __device__ __forceinline__ void wht_pass(R* arr, int L, int s, int ti, int nt) {
@@ -334,7 +402,7 @@ __global__ void __launch_bounds__(kBT, 1)
     Real acc[8], lo[8];  // FFT: Re/Im of 4 frequencies; FWHT: 8 frequencies
 #pragma unroll
     for (int j = 0; j < 8; ++j) { acc[j] = (Real)0; lo[j] = (Real)0; }
-    const bool tc = kF32 && !fft && logL >= 8;  // Hadamard-16 stages on the tensor cores
+    const bool tc = kF32 && !fft && logL >= 8 && P.tc;  // Hadamard-16 stages on the tensor cores
 
     for (int64_t k0 = kb; k0 < ke; k0 += KB) {
       const int64_t k = k0 + q;
@@ -416,10 +484,20 @@ __global__ void __launch_bounds__(kBT, 1)
         C* A = bufA(q);
         C* Bq = bufB(q);
         int s = 0;
-        if (P.radix == 8 && logL >= 3) fft_pass<8, true>(A, Bq, L, 0, wt, ti, NT), s = 3;
+        if (logL == 12 && P.radix == 8) {  // the common slab: strides fixed at compile time
+          fft_pass_fixed<8, true, 12, 0, NT>(A, Bq, wt, ti);
+          __syncthreads();
+          fft_pass_fixed<8, false, 12, 3, NT>(A, Bq, wt, ti);
+          __syncthreads();
+          fft_pass_fixed<8, false, 12, 6, NT>(A, Bq, wt, ti);
+          __syncthreads();
+          fft_pass_fixed<8, false, 12, 9, NT>(A, Bq, wt, ti);
+          __syncthreads();
+          s = logL;
+        } else if (P.radix == 8 && logL >= 3) fft_pass<8, true>(A, Bq, L, 0, wt, ti, NT), s = 3;
         else if (logL >= 2) fft_pass<4, true>(A, Bq, L, 0, wt, ti, NT), s = 2;
         else fft_pass<2, true>(A, Bq, L, 0, wt, ti, NT), s = 1;
-        __syncthreads();
+        if (s < logL || !(logL == 12 && P.radix == 8)) __syncthreads();
         if (P.radix == 8)
           for (; s + 3 <= logL; s += 3) { fft_pass<8, false>(A, Bq, L, s, wt, ti, NT); __syncthreads(); }
         for (; s + 2 <= logL; s += 2) { fft_pass<4, false>(A, Bq, L, s, wt, ti, NT); __syncthreads(); }
@@ -437,10 +515,21 @@ __global__ void __launch_bounds__(kBT, 1)
             }
           }
         }
-        if (P.radix == 8)
+        if (logL == 13 && P.radix == 8 && s == 0) {  // the common slab, strides fixed (FP64)
+          wht_pass_fixed<8, 13, 0, NT>(xs, ti); wht_pass_fixed<8, 13, 0, NT>(ys, ti); __syncthreads();
+          wht_pass_fixed<8, 13, 3, NT>(xs, ti); wht_pass_fixed<8, 13, 3, NT>(ys, ti); __syncthreads();
+          wht_pass_fixed<8, 13, 6, NT>(xs, ti); wht_pass_fixed<8, 13, 6, NT>(ys, ti); __syncthreads();
+          wht_pass_fixed<8, 13, 9, NT>(xs, ti); wht_pass_fixed<8, 13, 9, NT>(ys, ti); __syncthreads();
+          s = 12;
+        } else if (logL == 13 && s == 12) {  // after the tensor-core stages (FP32)
+        } else if (P.radix == 8)
           for (; s + 3 <= logL; s += 3) { wht_pass<8>(xs, L, s, ti, NT); wht_pass<8>(ys, L, s, ti, NT); __syncthreads(); }
         for (; s + 2 <= logL; s += 2) { wht_pass<4>(xs, L, s, ti, NT); wht_pass<4>(ys, L, s, ti, NT); __syncthreads(); }
-        if (s < logL) { wht_pass<2>(xs, L, s, ti, NT); wht_pass<2>(ys, L, s, ti, NT); __syncthreads(); }
+        if (logL == 13 && s == 12) {
+          wht_pass_fixed<2, 13, 12, NT>(xs, ti);
+          wht_pass_fixed<2, 13, 12, NT>(ys, ti);
+          __syncthreads();
+        } else if (s < logL) { wht_pass<2>(xs, L, s, ti, NT); wht_pass<2>(ys, L, s, ti, NT); __syncthreads(); }
       }
       // ---- accumulate over the row slots: thread tid owns m = tid + j kBT
       if (fft) {
@@ -558,7 +647,7 @@ struct TuneKey {
   }
 };
 struct TuneVal {
-  int logL, radix;
+  int logL, radix, tc;
 };
 std::mutex g_tune_mu;
 std::map<TuneKey, TuneVal> g_tune;  // process-wide autotuner cache
@@ -611,13 +700,14 @@ void batch_launch_sketch(bool f32, const BProd* dP, const BItem* dI, int n_items
   else launch_sketch<double>(dP, dI, n_items, dCounter, tw4096, ctas, s);
 }
 
-bool batch_tuned(int variant, bool f32, int log2b, int64_t n_ab, int* logL, int* radix) {
+bool batch_tuned(int variant, bool f32, int log2b, int64_t n_ab, int* logL, int* radix, int* tc) {
   const TuneKey key{variant, (int)f32, log2b, ilog2c(std::max<int64_t>(n_ab, 1))};
   std::lock_guard<std::mutex> g(g_tune_mu);
   auto it = g_tune.find(key);
   if (it == g_tune.end()) return false;
   *logL = it->second.logL;
   *radix = it->second.radix;
+  *tc = it->second.tc;
   return true;
 }
 
@@ -631,7 +721,7 @@ struct BatchPlan {
   std::vector<cmm_batch_product> prods;
   std::vector<SketchPlan> plans;  // slab geometry + k-groups per product (finalize)
   std::vector<SlabPlan> splans;   // per product: indices sorted by slab position
-  std::vector<int> radix, tuned;
+  std::vector<int> radix, tuned, tc;
   std::vector<const double2*> tw;  // w_b table per product
   std::vector<size_t> off_codesA, off_codesB, off_scale, off_partial;
   cudaStream_t stream = nullptr;  // creation stream (owns the buffers)
@@ -686,6 +776,7 @@ BProd make_bprod(const BatchPlan& B, int i, void* partial, const SlabPlan& sp) {
   d.G = P.G;
   d.variant = q.variant;
   d.radix = B.radix[(size_t)i];
+  d.tc = B.tc[(size_t)i];
   return d;
 }
 
@@ -745,10 +836,15 @@ TuneVal autotune(BatchPlan& B, int i, cudaStream_t s) {
   const int log2b = B.plans[(size_t)i].log2b;
   const int lmax = q.variant == kVariantFFT ? kBFftLog : kBWhtLog;
   std::vector<TuneVal> cand;
+  // FP32 FWHT also weighs the tensor-core Hadamard-16 stages against CUDA cores
+  const bool tc_choice = B.f32 && q.variant == kVariantFWHT;
   for (int dl = 0; dl < 3; ++dl) {
     const int logL = std::min(log2b, lmax) - dl;  // slab lengths L, L/2, L/4
     if (logL < 1) continue;
-    for (int rx : {8, 4}) cand.push_back({logL, rx});
+    for (int rx : {8, 4}) {
+      cand.push_back({logL, rx, 1});
+      if (tc_choice && logL >= 8) cand.push_back({logL, rx, 0});
+    }
   }
   const int64_t rows = std::min<int64_t>(q.n_inner, 96);
   float best_ms = 1e30f;
@@ -766,13 +862,15 @@ TuneVal autotune(BatchPlan& B, int i, cudaStream_t s) {
     DevBuf part((size_t)G * q.d * (size_t)q.b * (q.variant == kVariantFFT ? 16 : 8), s);
     const SlabPlan sp = make_sorted(B, i, c.logL, s);
     const SketchPlan keep = B.plans[(size_t)i];
-    const int keep_rx = B.radix[(size_t)i];
+    const int keep_rx = B.radix[(size_t)i], keep_tc = B.tc[(size_t)i];
     B.plans[(size_t)i] = P;
     B.radix[(size_t)i] = c.radix;
+    B.tc[(size_t)i] = c.tc;
     BProd bp = make_bprod(B, i, part.ptr, sp);
     bp.n_inner = rows;  // the first rows only
     B.plans[(size_t)i] = keep;
     B.radix[(size_t)i] = keep_rx;
+    B.tc[(size_t)i] = keep_tc;
     std::vector<BItem> its;
     for (int g = 0; g < G; ++g)
       for (int t = 0; t < q.d; ++t)
@@ -792,13 +890,16 @@ TuneVal autotune(BatchPlan& B, int i, cudaStream_t s) {
       CMM_CUDA(cudaEventElapsedTime(&t, e0, e1));
       if (rep > 0) ms = std::min(ms, t);  // the first launch warms up
     }
+    if (getenv("CMM_DEBUG"))
+      fprintf(stderr, "[cmm] batch tune candidate: variant=%d b=%d L=%d radix=%d tc=%d: %.3f ms\n", q.variant, q.b,
+              1 << c.logL, c.radix, c.tc, ms);
     if (ms < best_ms) { best_ms = ms; best = c; }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (getenv("CMM_DEBUG"))
-    fprintf(stderr, "[cmm] batch tune: variant=%d f32=%d b=%d n=%lld -> L=%d radix=%d (%.3f ms)\n", q.variant,
-            (int)B.f32, q.b, (long long)(q.n_a + q.n_b), 1 << best.logL, best.radix, best_ms);
+    fprintf(stderr, "[cmm] batch tune: variant=%d f32=%d b=%d n=%lld -> L=%d radix=%d tc=%d (%.3f ms)\n",
+            q.variant, (int)B.f32, q.b, (long long)(q.n_a + q.n_b), 1 << best.logL, best.radix, best.tc, best_ms);
   return best;
 }
 
@@ -842,6 +943,7 @@ BatchPlan* batch_create(const cmm_batch_product* products, int count, bool f32, 
   size_t ncodes = 0, nscale = 0;
   B->plans.resize((size_t)count);
   B->radix.assign((size_t)count, 8);
+  B->tc.assign((size_t)count, 1);
   B->tuned.assign((size_t)count, 0);
   B->tw.resize((size_t)count);
   B->off_codesA.resize((size_t)count);
@@ -912,7 +1014,7 @@ BatchPlan* batch_create(const cmm_batch_product* products, int count, bool f32, 
     const cmm_batch_product& q = B->prods[(size_t)i];
     SketchPlan& P = B->plans[(size_t)i];
     const TuneKey key{q.variant, (int)f32, P.log2b, ilog2c(std::max<int64_t>(q.n_a + q.n_b, 1))};
-    TuneVal v{P.logL, 8};
+    TuneVal v{P.logL, 8, 1};
     bool have = false;
     {
       std::lock_guard<std::mutex> g(g_tune_mu);
@@ -927,6 +1029,7 @@ BatchPlan* batch_create(const cmm_batch_product* products, int count, bool f32, 
     }
     set_geometry(P, v.logL);
     B->radix[(size_t)i] = v.radix;
+    B->tc[(size_t)i] = v.tc;
     B->tuned[(size_t)i] = have ? 1 : 0;
   }
 

@@ -29,6 +29,7 @@ struct BProd {
   int64_t n_a, n_inner, n_b;
   int SA, SB, code16;
   int d, log2b, logL, logR, G, variant, radix;
+  int tc;  // FP32 FWHT: Hadamard-16 stages on the tensor cores (else CUDA cores)
 };
 // one work item: (product, repetition t, slab r, k-group g)
 struct BItem {
@@ -41,7 +42,7 @@ int batch_resident_ctas(bool f32);
 void batch_launch_sketch(bool f32, const BProd* dP, const BItem* dI, int n_items, int* dCounter,
                          const double2* tw4096, int ctas, cudaStream_t s);
 // the autotuner's cached (slab length, radix) for a product class, if any
-bool batch_tuned(int variant, bool f32, int log2b, int64_t n_ab, int* logL, int* radix);
+bool batch_tuned(int variant, bool f32, int log2b, int64_t n_ab, int* logL, int* radix, int* tc);
 // relative cost of one (t, slab, row) unit
 double batch_unit_cost(int64_t n_a, int64_t n_b, int logL);
 

@@ -69,7 +69,7 @@ struct Request {
   cmm_request r{};
   Clock::time_point t_submit, t_done;
   size_t need = 0;
-  int log2b = 0, logL = 0, radix = 8, G = 1;
+  int log2b = 0, logL = 0, radix = 8, tc = 1, G = 1;
   bool done = false;
   std::string error;
   // device state (allocated on the upload stream at admission)
@@ -132,14 +132,16 @@ void geometry(Request& q, bool f32) {
   const cmm_request& r = q.r;
   q.log2b = ilog2i(r.b);
   const int lmax = r.variant == kVariantFFT ? kBatchFftLog : kBatchWhtLog;
-  int logL = std::min(q.log2b, lmax), radix = 8;
-  int tl = 0, tr = 0;
-  if (batch_tuned(r.variant, f32, q.log2b, r.n_a + r.n_b, &tl, &tr)) {
+  int logL = std::min(q.log2b, lmax), radix = 8, tc = 1;
+  int tl = 0, tr = 0, tt = 1;
+  if (batch_tuned(r.variant, f32, q.log2b, r.n_a + r.n_b, &tl, &tr, &tt)) {
     logL = tl;
     radix = tr;
+    tc = tt;
   }
   q.logL = logL;
   q.radix = radix;
+  q.tc = tc;
   // items of about the cost of 64 rows of a 2048 + 2048 product at L = 4096
   const double target = 64.0 * batch_unit_cost(2048, 2048, 12);
   const double row = batch_unit_cost(r.n_a, r.n_b, logL);
@@ -246,6 +248,7 @@ BProd bprod(const Request& q) {
   d.G = q.G;
   d.variant = q.r.variant;
   d.radix = q.radix;
+  d.tc = q.tc;
   return d;
 }
 
