@@ -593,6 +593,105 @@ __global__ void __launch_bounds__(kBT, 1)
   }
 }
 
+// ---------------------------------------------------------- batched finalize
+// One CTA per (product, repetition t) with b <= 2^14: the k-group reduction
+// of the slab partials and the inverse transform in shared memory, in FP64.
+// FFT: P[f] = (Q[f] - conj(Q[-f])) / (4i) is the spectrum of the real p;
+// p is recovered from a half-length complex inverse of
+//   Z[k] = (P[k] + P[k + b/2]) + i (P[k] - P[k + b/2]) w_b^{-k},  k < b/2,
+// whose output is z[n] = b (p[2n] + i p[2n+1]).  FWHT: p = WHT_b(P) / b.
+constexpr int kFinThreads = 1024;
+
+__global__ void __launch_bounds__(kFinThreads, 1) k_finalize_jobs(const FinJob* __restrict__ jobs) {
+  const FinJob J = jobs[blockIdx.x];
+  extern __shared__ __align__(16) unsigned char sfin[];
+  const int tid = threadIdx.x;
+  const int b = 1 << J.log2b, L = 1 << J.logL, logR = J.log2b - J.logL, R = 1 << logR;
+  if (J.variant == kVariantFFT) {
+    const double2* part = reinterpret_cast<const double2*>(J.partial);
+    const size_t gstride = (size_t)J.d * (size_t)b;
+    const size_t tbase = (size_t)J.t * (size_t)b;
+    auto Q = [&](int f) {  // sum over k-groups at frequency f = R m + r
+      const size_t off = tbase + ((size_t)(f & (R - 1)) << J.logL) + (size_t)(f >> logR);
+      double2 q = make_double2(0.0, 0.0);
+      for (int g = 0; g < J.G; ++g) {
+        const double2 v = part[(size_t)g * gstride + off];
+        q.x += v.x;
+        q.y += v.y;
+      }
+      return q;
+    };
+    auto P = [&](int f) {
+      const double2 q = Q(f), qn = Q((b - f) & (b - 1));
+      return make_double2(0.25 * (q.y + qn.y), -0.25 * (q.x - qn.x));
+    };
+    const int logM = J.log2b - 1, M = 1 << logM;
+    double2* z = reinterpret_cast<double2*>(sfin);
+    for (int k = tid; k < M; k += kFinThreads) {
+      const double2 x0 = P(k), x1 = P(k + M);
+      const double2 w = J.tw[k];  // w_b^k; the conjugate is used
+      const double dx = x0.x - x1.x, dy = x0.y - x1.y;
+      const double ex = dx * w.x + dy * w.y, ey = dy * w.x - dx * w.y;  // (x0 - x1) conj(w)
+      z[ph<16>((int)brev_bits((uint32_t)k, logM))] = make_double2(x0.x + x1.x - ey, x0.y + x1.y + ex);
+    }
+    __syncthreads();
+    for (int st = 0; st < logM; ++st) {  // inverse DIT, conjugate twiddles
+      const int half = 1 << st;
+      for (int p = tid; p < (M >> 1); p += kFinThreads) {
+        const int kk = p & (half - 1);
+        const int ia = ((p >> st) << (st + 1)) | kk, ic = ia + half;
+        const double2 w = J.tw[(size_t)kk << (J.log2b - st - 1)];
+        const double2 u = z[ph<16>(ia)], v = z[ph<16>(ic)];
+        const double2 vw = make_double2(v.x * w.x + v.y * w.y, v.y * w.x - v.x * w.y);
+        z[ph<16>(ia)] = make_double2(u.x + vw.x, u.y + vw.y);
+        z[ph<16>(ic)] = make_double2(u.x - vw.x, u.y - vw.y);
+      }
+      __syncthreads();
+    }
+    const double inv = 1.0 / (double)b;
+    for (int n = tid; n < M; n += kFinThreads) {
+      const double2 v = z[ph<16>(n)];
+      J.p[(size_t)J.t * b + 2 * n] = v.x * inv;
+      J.p[(size_t)J.t * b + 2 * n + 1] = v.y * inv;
+    }
+  } else {
+    const double* part = reinterpret_cast<const double*>(J.partial);
+    const size_t gstride = (size_t)J.d * (size_t)b;
+    double* x = reinterpret_cast<double*>(sfin);
+    for (int f = tid; f < b; f += kFinThreads) {  // f = r L + m is the slab layout itself
+      double q = 0.0;
+      for (int g = 0; g < J.G; ++g) q += part[(size_t)g * gstride + (size_t)J.t * b + f];
+      x[ph<8>(f)] = q;
+    }
+    __syncthreads();
+    for (int st = 0; st < J.log2b; ++st) {
+      const int half = 1 << st;
+      for (int p = tid; p < (b >> 1); p += kFinThreads) {
+        const int ia = ((p >> st) << (st + 1)) | (p & (half - 1)), ic = ia + half;
+        const double u = x[ph<8>(ia)], v = x[ph<8>(ic)];
+        x[ph<8>(ia)] = u + v;
+        x[ph<8>(ic)] = u - v;
+      }
+      __syncthreads();
+    }
+    const double inv = 1.0 / (double)b;
+    for (int f = tid; f < b; f += kFinThreads) J.p[(size_t)J.t * b + f] = x[ph<8>(f)] * inv;
+  }
+  (void)L;
+}
+
+bool batch_finalize_fits(int log2b) { return log2b >= 2 && log2b <= 14; }
+
+void batch_launch_finalize(const FinJob* dJobs, int n_jobs, cudaStream_t s) {
+  if (n_jobs <= 0) return;
+  const size_t smem = 147456;  // 2^13 complex FP64 (or 2^14 real) + padding
+  CMM_CUDA(cudaFuncSetAttribute(k_finalize_jobs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  ProfScope prof("finalize", s);
+  count_launch();
+  k_finalize_jobs<<<(unsigned)n_jobs, kFinThreads, smem, s>>>(dJobs);
+  CMM_CUDA(cudaGetLastError());
+}
+
 // per-k exponent balance of many products (FFT): the same rule as the
 // single-product kernels (k_row_scale / k_row_scale_f32)
 struct ScaleJob {
@@ -725,7 +824,8 @@ struct BatchPlan {
   std::vector<const double2*> tw;  // w_b table per product
   std::vector<size_t> off_codesA, off_codesB, off_scale, off_partial;
   cudaStream_t stream = nullptr;  // creation stream (owns the buffers)
-  DevBuf params, codes, scale, partial, work, dprods, ditems, counter, hjobs, sjobs;
+  DevBuf params, codes, scale, partial, work, dprods, ditems, counter, hjobs, sjobs, fjobs;
+  int n_fjobs = 0;  // batched finalize jobs (b <= 2^14); other products finalize one by one
   int n_items = 0, ctas = 0, n_scale_jobs = 0;
   int64_t max_hash_total = 0, max_inner = 0;
   const double2* tw4096 = nullptr;
@@ -819,10 +919,12 @@ void enqueue(BatchPlan& B, cudaStream_t s) {
       launch_sketch<double>(B.dprods.as<BProd>(), B.ditems.as<BItem>(), B.n_items, B.counter.as<int>(),
                             B.tw4096, B.ctas, s);
   }
+  batch_launch_finalize(B.fjobs.as<FinJob>(), B.n_fjobs, s);
   for (int i = 0; i < B.count; ++i) {
     const cmm_batch_product& q = B.prods[(size_t)i];
-    launch_finalize(B.plans[(size_t)i], B.partial.as<unsigned char>() + B.off_partial[(size_t)i], B.tw[(size_t)i],
-                    B.work.ptr, q.p, s);
+    if (!batch_finalize_fits(B.plans[(size_t)i].log2b))
+      launch_finalize(B.plans[(size_t)i], B.partial.as<unsigned char>() + B.off_partial[(size_t)i], B.tw[(size_t)i],
+                      B.work.ptr, q.p, s);
     if (q.C)
       launch_decompress_dense(q.variant, q.d, q.b, q.n_a, q.n_b, B.codes.as<uint32_t>() + B.off_codesA[(size_t)i],
                               B.codes.as<uint32_t>() + B.off_codesB[(size_t)i], q.p, q.C, s);
@@ -1081,6 +1183,17 @@ BatchPlan* batch_create(const cmm_batch_product* products, int count, bool f32, 
   }
   std::vector<BItem> bi;
   for (const Cost& c : items) bi.push_back(c.it);
+  std::vector<FinJob> fj;
+  for (int i = 0; i < count; ++i) {
+    const SketchPlan& P = B->plans[(size_t)i];
+    if (!batch_finalize_fits(P.log2b)) continue;
+    for (int t = 0; t < P.d; ++t)
+      fj.push_back({B->partial.as<unsigned char>() + B->off_partial[(size_t)i], B->prods[(size_t)i].p, B->tw[(size_t)i],
+                    P.G, P.d, t, P.log2b, P.logL, P.variant});
+  }
+  B->n_fjobs = (int)fj.size();
+  B->fjobs = DevBuf(std::max<size_t>(fj.size(), 1) * sizeof(FinJob), s);
+  if (!fj.empty()) CMM_CUDA(cudaMemcpyAsync(B->fjobs.ptr, fj.data(), fj.size() * sizeof(FinJob), cudaMemcpyHostToDevice, s));
   B->dprods = DevBuf(std::max<size_t>(bp.size(), 1) * sizeof(BProd), s);
   B->ditems = DevBuf(std::max<size_t>(bi.size(), 1) * sizeof(BItem), s);
   if (!bp.empty()) CMM_CUDA(cudaMemcpyAsync(B->dprods.ptr, bp.data(), bp.size() * sizeof(BProd), cudaMemcpyHostToDevice, s));
@@ -1127,9 +1240,13 @@ void batch_info(const BatchPlan* B, int64_t* items, int* ctas, int* launches) {
   if (items) *items = B->n_items;
   if (ctas) *ctas = B->ctas;
   if (launches) {
-    // kernels per run: scale (if any), sketch (if any), 3 per finalize, 1 per dense C
-    int n = (B->n_scale_jobs ? 1 : 0) + (B->n_items ? 1 : 0);
-    for (const auto& q : B->prods) n += 3 + (q.C && q.n_a > 0 && q.n_b > 0 ? 1 : 0);
+    // kernels per run: scale (if any), sketch (if any), the batched finalize,
+    // 3 per other finalize, 1 per dense C
+    int n = (B->n_scale_jobs ? 1 : 0) + (B->n_items ? 1 : 0) + (B->n_fjobs ? 1 : 0);
+    for (size_t i = 0; i < B->prods.size(); ++i) {
+      const auto& q = B->prods[i];
+      n += (batch_finalize_fits(B->plans[i].log2b) ? 0 : 3) + (q.C && q.n_a > 0 && q.n_b > 0 ? 1 : 0);
+    }
     *launches = n;
   }
 }

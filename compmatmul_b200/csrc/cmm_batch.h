@@ -36,6 +36,18 @@ struct BItem {
   int prod, t, r, g;
 };
 
+// one (product, repetition) of the batched k-group reduction + inverse
+struct FinJob {
+  const void* partial;  // [G][d][R][L] slab partials
+  double* p;            // d x b sketch (row t written)
+  const double2* tw;    // w_b^j, j < b
+  int G, d, t, log2b, logL, variant;
+};
+// b in [4, 2^14]: the inverse fits one CTA's shared memory
+bool batch_finalize_fits(int log2b);
+// one launch over n_jobs jobs
+void batch_launch_finalize(const FinJob* dJobs, int n_jobs, cudaStream_t s);
+
 // CTAs of the persistent kernel that fit the device at once
 int batch_resident_ctas(bool f32);
 // one persistent launch over n_items items (counter: one device int, reset here)

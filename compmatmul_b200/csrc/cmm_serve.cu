@@ -85,8 +85,8 @@ struct Request {
 struct Wave {
   std::vector<std::shared_ptr<Request>> reqs;
   int stream = 0;
-  DevBuf dprods, ditems, counter;
-  void* host = nullptr;  // pinned staging of the item / product tables
+  DevBuf dprods, counter;  // dprods: products | items | finalize jobs
+  void* host = nullptr;      // pinned staging of those tables
   size_t host_cls = 0;
   cudaEvent_t done = nullptr;
 };
@@ -274,22 +274,32 @@ void launch_wave(Server& S, std::vector<std::shared_ptr<Request>> reqs, int si) 
     }
   }
   std::stable_sort(items.begin(), items.end(), [](const C& a, const C& b) { return a.c > b.c; });
-  const size_t pb = prods.size() * sizeof(BProd), ib = items.size() * sizeof(BItem);
-  W->host = S.pinned.get(std::max<size_t>(pb + ib, 16), &W->host_cls);
-  std::memcpy(W->host, prods.data(), pb);
-  BItem* hi = reinterpret_cast<BItem*>(static_cast<unsigned char*>(W->host) + pb);
+  std::vector<FinJob> fin;  // one batched reduction + inverse for the small-b requests
+  for (auto& qp : reqs)
+    if (batch_finalize_fits(qp->log2b))
+      for (int t = 0; t < qp->r.d; ++t)
+        fin.push_back({qp->partial.ptr, qp->p_dev.as<double>(), qp->tw, qp->G, qp->r.d, t, qp->log2b, qp->logL,
+                       qp->r.variant});
+  // one pinned staging block and one device table: products | items | finalize jobs
+  const size_t pb = prods.size() * sizeof(BProd), ib = items.size() * sizeof(BItem), fb = fin.size() * sizeof(FinJob);
+  const size_t ioff = (pb + 15) & ~(size_t)15, foff = (ioff + ib + 15) & ~(size_t)15, total = foff + fb;
+  W->host = S.pinned.get(std::max<size_t>(total, 16), &W->host_cls);
+  unsigned char* hb = static_cast<unsigned char*>(W->host);
+  std::memcpy(hb, prods.data(), pb);
+  BItem* hi = reinterpret_cast<BItem*>(hb + ioff);
   for (size_t i = 0; i < items.size(); ++i) hi[i] = items[i].it;
-  W->dprods = DevBuf(std::max<size_t>(pb, 16), s);
-  W->ditems = DevBuf(std::max<size_t>(ib, 16), s);
+  if (fb) std::memcpy(hb + foff, fin.data(), fb);
+  W->dprods = DevBuf(std::max<size_t>(total, 16), s);
   W->counter = DevBuf(sizeof(int), s);
-  CMM_CUDA(cudaMemcpyAsync(W->dprods.ptr, W->host, pb, cudaMemcpyHostToDevice, s));
-  if (ib) CMM_CUDA(cudaMemcpyAsync(W->ditems.ptr, hi, ib, cudaMemcpyHostToDevice, s));
+  CMM_CUDA(cudaMemcpyAsync(W->dprods.ptr, hb, total, cudaMemcpyHostToDevice, s));
+  unsigned char* db = W->dprods.as<unsigned char>();
   const int n_items = (int)items.size();
-  batch_launch_sketch(S.cfg.f32 != 0, W->dprods.as<BProd>(), W->ditems.as<BItem>(), n_items, W->counter.as<int>(),
-                      S.tw4096, std::max(1, std::min(S.ctas, n_items)), s);
+  batch_launch_sketch(S.cfg.f32 != 0, reinterpret_cast<const BProd*>(db), reinterpret_cast<const BItem*>(db + ioff),
+                      n_items, W->counter.as<int>(), S.tw4096, std::max(1, std::min(S.ctas, n_items)), s);
+  batch_launch_finalize(reinterpret_cast<const FinJob*>(db + foff), (int)fin.size(), s);
   for (auto& qp : reqs) {
     Request& q = *qp;
-    launch_finalize(q.sp, q.partial.ptr, q.tw, q.work.ptr, q.p_dev.as<double>(), s);
+    if (!batch_finalize_fits(q.log2b)) launch_finalize(q.sp, q.partial.ptr, q.tw, q.work.ptr, q.p_dev.as<double>(), s);
     CMM_CUDA(cudaMemcpyAsync(q.stage, q.p_dev.ptr, q.p_dev.bytes, cudaMemcpyDeviceToHost, s));
   }
   CMM_CUDA(cudaEventCreateWithFlags(&W->done, cudaEventDisableTiming));
