@@ -84,9 +84,26 @@ def build_module(verbose=False):
     return target
 
 
+CLI = os.path.join(PKG, "cmm_multiply")
+
+
+def build_cli(verbose=False):
+    """The `multiply` command-line program (csrc/multiply_main.cpp)."""
+    src = os.path.join(CSRC, "multiply_main.cpp")
+    if not _stale(CLI, [src, LIB, os.path.join(INCLUDE, "compmatmul_b200.h")]):
+        return CLI
+    cuda = os.path.dirname(os.path.dirname(NVCC)) if os.path.isabs(NVCC) else "/usr/local/cuda"
+    cmd = ["g++", "-std=c++17", "-O2", "-I" + INCLUDE, "-I" + os.path.join(cuda, "include"), src, "-o", CLI,
+           "-L" + PKG, "-l:libcmm_b200.so", "-L" + os.path.join(cuda, "lib64"), "-lcudart",
+           "-Wl,-rpath,$ORIGIN", "-Wl,-rpath," + os.path.join(cuda, "lib64")]
+    _run(cmd, verbose)
+    return CLI
+
+
 def build(verbose=False):
     build_lib(verbose)
     build_module(verbose)
+    build_cli(verbose)
 
 
 if __name__ == "__main__":
