@@ -235,13 +235,8 @@ def bench_batch(args, world, rank, local):
     import compmatmul_b200 as cmb
     from compmatmul_b200 import device as dev
     from compmatmul_b200.batch import BatchPlan
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-    else:
-        torch.cuda.set_device(0)
+    from compmatmul_b200.replicas import Replicas
+    reps = Replicas()
     L = cmb.lib()
     prods, planted = [], []
     for s in shapes:
@@ -255,11 +250,7 @@ def bench_batch(args, world, rank, local):
         plan.run()
     torch.cuda.synchronize()
 
-    def barrier():
-        if world > 1:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
-
+    barrier = reps.barrier
     clocks = ClockSampler(torch.cuda.current_device())
     L.cmm_profile_reset()
     L.cmm_profile_enable(1)
@@ -277,12 +268,9 @@ def bench_batch(args, world, rank, local):
     launches = L.cmm_launch_count() - launches0
     L.cmm_profile_enable(0)
     total_ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    total_ms = float(t.item())
+    value = reps.throughput(count * args.steps, total_ms / 1e3)
+    total_ms = reps.max(total_ms)
     ms_per_step = total_ms / args.steps
-    value = world * count * args.steps / (total_ms / 1e3)
     info = plan.info()
 
     # the persistent sketch kernel alone (its own run, events on the same stream)
@@ -369,10 +357,7 @@ def bench_batch(args, world, rank, local):
         torch.cuda.synchronize()
     barrier()
     e2e_s = (time.perf_counter() - te0) / e2e_steps
-    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-    e2e_value = world * count / float(te.item())
+    e2e_value = reps.throughput(count, e2e_s)
 
     fma = C.c_double(0.0)
     fma_peak = fma.value if L.cmm_probe_fma_tflops(0, C.byref(fma)) == 0 else None
@@ -380,8 +365,7 @@ def bench_batch(args, world, rank, local):
     peak, peak_kind = measured_peaks()
     if rank != 0:
         plan.close()
-        if world > 1:
-            torch.distributed.destroy_process_group()
+        reps.close()
         return
     line = {
         "metric": METRIC, "value": value, "unit": "products/s", "n_gpus": world, "steps": args.steps,
@@ -410,8 +394,7 @@ def bench_batch(args, world, rank, local):
         line["plain_fp64_same_inputs"] = fp64
     print(json.dumps(line), flush=True)
     plan.close()
-    if world > 1:
-        torch.distributed.destroy_process_group()
+    reps.close()
 
 
 # ------------------------------------------------------------ serving (config 5)
@@ -587,14 +570,9 @@ def main():
     import torch
     import compmatmul_b200 as cmb
     from compmatmul_b200 import device as dev
+    from compmatmul_b200.replicas import Replicas
 
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-    else:
-        torch.cuda.set_device(0)
+    reps = Replicas()
     L = cmb.lib()
     dv = torch.device("cuda", torch.cuda.current_device())
 
@@ -616,11 +594,7 @@ def main():
         step()
     torch.cuda.synchronize()
 
-    def barrier():
-        if world > 1:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
-
+    barrier = reps.barrier
     clocks = ClockSampler(torch.cuda.current_device())
     L.cmm_profile_reset()
     L.cmm_profile_enable(1)
@@ -641,12 +615,9 @@ def main():
     fam = {f: cmb.profile_read(f) for f in ("hash", "scale", "plan", "materialize", "sketch",
                                              "finalize", "decompress", "topk")}
     sketch_kernel = L.cmm_last_sketch_kernel().decode()
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dv)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    total_ms = float(t.item())
+    value = reps.throughput(args.steps, total_ms / 1e3)  # products of all ranks / slowest rank
+    total_ms = reps.max(total_ms)
     ms_per_step = total_ms / args.steps
-    value = world * args.steps / (total_ms / 1e3)
 
     # recovery check on this rank's last step (planted entries should be the top-K)
     ti, tj, tv = [x.cpu().numpy() for x in out]
@@ -666,10 +637,7 @@ def main():
         cmb.check(st)
     barrier()
     e2e_s = (time.perf_counter() - te0) / e2e_steps
-    te = torch.tensor([e2e_s], dtype=torch.float64, device=dv)
-    if world > 1:
-        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-    e2e_value = world / float(te.item())
+    e2e_value = reps.throughput(1, e2e_s)
 
     # the plain FP64 path on the same (FP32-valued) inputs, for the mixed speed-up
     fp64_ms = None
@@ -706,8 +674,7 @@ def main():
         fma_peak = tf.value
 
     if rank != 0:
-        if world > 1:
-            torch.distributed.destroy_process_group()
+        reps.close()
         return
 
     cpu = None
@@ -749,8 +716,7 @@ def main():
     if fp64_ms is not None:
         line["plain_fp64_same_inputs"] = {"ms_per_step": fp64_ms, "speedup": fp64_ms / ms_per_step}
     print(json.dumps(line), flush=True)
-    if world > 1:
-        torch.distributed.destroy_process_group()
+    reps.close()
 
 
 if __name__ == "__main__":
