@@ -38,7 +38,8 @@ EXPORTED = [
     "cmm_compressed_product_f32", "cmm_matmul_f32", "cmm_dev_compressed_product_noalloc",
     "cmm_last_sketch_kernel", "cmm_probe_fma_tflops", "cmm_batch_create", "cmm_batch_run",
     "cmm_batch_info", "cmm_batch_config", "cmm_batch_destroy", "cmm_server_create", "cmm_server_submit",
-    "cmm_server_wait", "cmm_server_stats_get", "cmm_server_destroy",
+    "cmm_server_wait", "cmm_server_stats_get", "cmm_server_destroy", "cmm_dev_decompress_entries",
+    "cmm_dev_sketch_topk",
 ]
 
 
@@ -78,6 +79,8 @@ def lib():
     L.cmm_server_wait.argtypes = [vp, u64, _C.c_double, _C.POINTER(_C.c_int), _C.POINTER(_C.c_double)]
     L.cmm_server_stats_get.argtypes = [vp, vp]
     L.cmm_server_destroy.argtypes = [vp]
+    L.cmm_dev_decompress_entries.argtypes = [i32, i32, i32, i32, u64, dp, i64, vp, vp, dp, vp]
+    L.cmm_dev_sketch_topk.argtypes = [i32, i32, i64, i64, i32, i32, u64, dp, i32, _C.c_size_t, vp, vp, dp, vp]
     L.cmm_device_count.restype = i32
     L.cmm_max_buckets.restype = i32
     L.cmm_matmul.argtypes = [i32, i32, i64, i64, i64, dp, dp, dp, i32, i32, i32, u64]

@@ -4,6 +4,7 @@
 // host (bit-exact with hashing.hpp), and runs the device pipeline:
 //   hash codes -> row balance (FFT) -> fused sketch/transform/accumulate
 //   -> k-group reduction + inverse -> (median decompression) -> (top-K).
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -639,6 +640,91 @@ int cmm_dev_topk(const double* dC, int64_t n_a, int64_t n_b, int K, uint32_t* d_
   return guarded([&] {
     if (n_a < 0 || n_b < 0 || K < 0) throw cmm::invalid_argument("negative size");
     topk_dense(dC, n_a, n_b, K, d_i, d_j, d_v, (cudaStream_t)stream);
+  });
+}
+
+int cmm_dev_decompress_entries(int variant, int hash_kind, int d, int b, uint64_t seed, const double* dP,
+                               int64_t count, const uint32_t* dI, const uint32_t* dJ, double* dOut,
+                               void* stream) {
+  return guarded([&] {
+    check_params(variant, hash_kind, d, b);
+    if (count < 0) throw cmm::invalid_argument("negative count");
+    if (count == 0) return;
+    cudaStream_t s = (cudaStream_t)stream;
+    SketchParams sp = make_sketch_params(hash_kind, d, b, seed);
+    DevBuf params = upload(sp.blob.data(), sp.blob.size(), s);
+    const size_t set = sp.fn_bytes * (size_t)d;
+    const uint8_t* base = params.as<uint8_t>();
+    DevBuf cI((size_t)d * count * 4, s), cJ((size_t)d * count * 4, s);
+    launch_hash_codes_keys(hash_kind, base, base + 2 * set, d, sp.log2b, count, dI, cI.as<uint32_t>(), s);
+    launch_hash_codes_keys(hash_kind, base + set, base + 3 * set, d, sp.log2b, count, dJ, cJ.as<uint32_t>(), s);
+    launch_decompress_list(variant, d, b, count, cI.as<uint32_t>(), cJ.as<uint32_t>(), dP, dOut, s);
+  });
+}
+
+int cmm_dev_sketch_topk(int variant, int hash_kind, int64_t n_a, int64_t n_b, int d, int b, uint64_t seed,
+                        const double* dP, int K, size_t scratch_bytes, uint32_t* d_i, uint32_t* d_j, double* d_v,
+                        void* stream) {
+  return guarded([&] {
+    check_params(variant, hash_kind, d, b);
+    check_sizes(n_a, 0, n_b);
+    if (K < 0) throw cmm::invalid_argument("negative K");
+    if (K == 0) return;
+    if ((int64_t)K > n_a * n_b) throw cmm::invalid_argument("K exceeds the number of entries");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (scratch_bytes == 0) scratch_bytes = (size_t)256 << 20;
+    // rows per tile: the tile's dense estimate fits the scratch and holds >= K entries
+    int64_t rows = (int64_t)(scratch_bytes / (8 * (size_t)n_b));
+    rows = std::max<int64_t>(rows, ((int64_t)K + n_b - 1) / n_b);
+    rows = std::min<int64_t>(std::max<int64_t>(rows, 1), n_a);
+    SketchParams sp = make_sketch_params(hash_kind, d, b, seed);
+    DevBuf params = upload(sp.blob.data(), sp.blob.size(), s);
+    const size_t set = sp.fn_bytes * (size_t)d;
+    const uint8_t* base = params.as<uint8_t>();
+    DevBuf cB((size_t)d * (size_t)n_b * 4, s);
+    launch_hash_codes(hash_kind, base + set, base + 3 * set, d, sp.log2b, n_b, cB.as<uint32_t>(), s);
+    DevBuf tile((size_t)rows * (size_t)n_b * 8, s), keys((size_t)rows * 4, s), cA((size_t)d * (size_t)rows * 4, s);
+    DevBuf ti((size_t)K * 4, s), tj((size_t)K * 4, s), tv((size_t)K * 8, s);
+    struct Cand { double v; uint64_t idx; };
+    std::vector<Cand> cand;
+    std::vector<uint32_t> hi((size_t)K), hj((size_t)K), hk((size_t)rows);
+    std::vector<double> hv((size_t)K);
+    for (int64_t i0 = 0; i0 < n_a; i0 += rows) {
+      const int64_t r = std::min<int64_t>(rows, n_a - i0);
+      for (int64_t e = 0; e < r; ++e) hk[(size_t)e] = (uint32_t)(i0 + e);
+      CMM_CUDA(cudaMemcpyAsync(keys.ptr, hk.data(), (size_t)r * 4, cudaMemcpyHostToDevice, s));
+      launch_hash_codes_keys(hash_kind, base, base + 2 * set, d, sp.log2b, r, keys.as<uint32_t>(),
+                             cA.as<uint32_t>(), s);
+      launch_decompress_dense(variant, d, b, r, n_b, cA.as<uint32_t>(), cB.as<uint32_t>(), dP, tile.as<double>(), s);
+      const int kt = (int)std::min<int64_t>(K, r * n_b);
+      topk_dense(tile.as<double>(), r, n_b, kt, ti.as<uint32_t>(), tj.as<uint32_t>(), tv.as<double>(), s);
+      CMM_CUDA(cudaMemcpyAsync(hi.data(), ti.ptr, (size_t)kt * 4, cudaMemcpyDeviceToHost, s));
+      CMM_CUDA(cudaMemcpyAsync(hj.data(), tj.ptr, (size_t)kt * 4, cudaMemcpyDeviceToHost, s));
+      CMM_CUDA(cudaMemcpyAsync(hv.data(), tv.ptr, (size_t)kt * 8, cudaMemcpyDeviceToHost, s));
+      CMM_CUDA(cudaStreamSynchronize(s));
+      for (int e = 0; e < kt; ++e)
+        cand.push_back({hv[(size_t)e], (uint64_t)(i0 + hi[(size_t)e]) * (uint64_t)n_b + hj[(size_t)e]});
+    }
+    // the tiles' top-K lists contain the global top-K under the same order:
+    // value descending (the device order of the bit keys), then (i, j)
+    auto key = [](double v) {
+      uint64_t b;
+      std::memcpy(&b, &v, 8);
+      return (b >> 63) ? ~b : (b | 0x8000000000000000ULL);
+    };
+    std::sort(cand.begin(), cand.end(), [&](const Cand& a, const Cand& c) {
+      const uint64_t ka = key(a.v), kc = key(c.v);
+      return ka != kc ? ka > kc : a.idx < c.idx;
+    });
+    for (int e = 0; e < K; ++e) {
+      hi[(size_t)e] = (uint32_t)(cand[(size_t)e].idx / (uint64_t)n_b);
+      hj[(size_t)e] = (uint32_t)(cand[(size_t)e].idx % (uint64_t)n_b);
+      hv[(size_t)e] = cand[(size_t)e].v;
+    }
+    CMM_CUDA(cudaMemcpyAsync(d_i, hi.data(), (size_t)K * 4, cudaMemcpyHostToDevice, s));
+    CMM_CUDA(cudaMemcpyAsync(d_j, hj.data(), (size_t)K * 4, cudaMemcpyHostToDevice, s));
+    CMM_CUDA(cudaMemcpyAsync(d_v, hv.data(), (size_t)K * 8, cudaMemcpyHostToDevice, s));
+    CMM_CUDA(cudaStreamSynchronize(s));
   });
 }
 

@@ -144,6 +144,21 @@ int cmm_dev_compressed_product_noalloc(int variant, int hash_kind, int64_t n_a, 
                                        int64_t n_b, const double* dAT, const double* dB, int d,
                                        int b, uint64_t seed, double* dP, void* stream);
 
+/* Device-resident sketch queries (matmul_decompress_fft/fwht on a device
+ * sketch, matmul_fft.hpp:135-147 / matmul_fwht.hpp:122-134): the median
+ * estimate of `count` listed entries (dI[e], dJ[e]) into dOut. */
+int cmm_dev_decompress_entries(int variant, int hash_kind, int d, int b, uint64_t seed, const double* dP,
+                               int64_t count, const uint32_t* dI, const uint32_t* dJ, double* dOut,
+                               void* stream);
+/* Top-K entries of the n_a x n_b median estimate of sketch dP without the
+ * dense matrix: rows are decompressed in tiles of at most scratch_bytes
+ * (0: 256 MiB; at least K entries), each tile's top-K is kept and the lists
+ * are merged.  Same result and order as cmm_dev_topk on the dense estimate
+ * (value descending, ties by (i, j) ascending).  K <= 4096; synchronises. */
+int cmm_dev_sketch_topk(int variant, int hash_kind, int64_t n_a, int64_t n_b, int d, int b, uint64_t seed,
+                        const double* dP, int K, size_t scratch_bytes, uint32_t* d_i, uint32_t* d_j, double* d_v,
+                        void* stream);
+
 /* Dense median decompression of dP into dC (n_a x n_b FP64). */
 int cmm_dev_decompress_dense(int variant, int hash_kind, int64_t n_a, int64_t n_b, int d, int b,
                              uint64_t seed, const double* dP, double* dC, void* stream);
