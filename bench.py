@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--serve-cap-gb", type=float, default=40.0, help="config5: admission cap (GB)")
     ap.add_argument("--serve-streams", type=int, default=4, help="config5: waves in flight")
     ap.add_argument("--serve-max-wave", type=int, default=64, help="config5: requests per wave")
+    ap.add_argument("--serve-cache-gb", type=float, default=4.0,
+                    help="config5: resident hash codes + plans across requests (0: off)")
     ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"],
                     help="fp64 = plain path; mixed = FP32 inputs (default for config3)")
     return ap.parse_args()
@@ -444,7 +446,8 @@ def bench_serve(args, world, rank, local):
     config = {"workload": f"config5: Poisson arrivals at {rate:g} req/s for {secs:g} s; each request one compressed "
                           f"product sized as config4 (m, n, p log-uniform in [256, 4096], FP32, planted, "
                           f"b = next pow2 >= 256 K, d in {{5,7,9}}, FFT/FWHT 50/50) from a pool of "
-                          f"{args.batch_count} inputs; admission cap {args.serve_cap_gb:g} GB; result = sketch p",
+                          f"{args.batch_count} inputs; admission cap {args.serve_cap_gb:g} GB; resident hash codes + plans "
+                          f"{args.serve_cache_gb:g} GB; result = sketch p",
               "rate_per_s": rate, "seconds": secs, "cap_bytes": cap}
     if args.impl == "reference":
         if rank == 0:
@@ -464,11 +467,15 @@ def bench_serve(args, world, rank, local):
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
     L = cmb.lib()
 
-    def run(pool_, f32, arr, streams=args.serve_streams):
-        srv = Server(mem_cap_bytes=cap, f32=f32, streams=streams, max_wave=args.serve_max_wave)
-        warm = [srv.submit(q["AT"], q["B"], q["d"], q["b"], q["seed"], q["variant"]) for q in pool_[:8]]
+    def run(pool_, f32, arr, streams=args.serve_streams, cache=int(args.serve_cache_gb * (1 << 30))):
+        srv = Server(mem_cap_bytes=cap, f32=f32, streams=streams, max_wave=args.serve_max_wave, cache_bytes=cache)
+        # warm-up: one burst of the whole pool fills the pinned staging and
+        # device pools (and, when enabled, the code/plan residency)
+        warm = [srv.submit(q["AT"], q["B"], q["d"], q["b"], q["seed"], q["variant"]) for q in pool_]
         for w in warm:
             srv.result(w)
+        serve_stream(srv, pool_, arr[arr < 1.0])  # one untimed second of the same stream
+        st0 = srv.stats()
         l0 = L.cmm_launch_count()
         clocks = ClockSampler(torch.cuda.current_device())
         clocks.start()
@@ -476,14 +483,18 @@ def bench_serve(args, world, rank, local):
         clk = clocks.stop()
         st = srv.stats()
         srv.close()
-        return {"products_per_s": len(lat) / span, "p50_ms": float(np.percentile(lat, 50) * 1e3),
+        return {"products_per_s": len(lat) / span, "cache_bytes": cache,
+                "cache_hits": int(st["cache_hits"] - st0["cache_hits"]),
+                "cache_misses": int(st["cache_misses"] - st0["cache_misses"]), "p50_ms": float(np.percentile(lat, 50) * 1e3),
                 "p99_ms": float(np.percentile(lat, 99) * 1e3), "mean_ms": float(lat.mean() * 1e3),
-                "requests": int(len(lat)), "span_s": span, "waves": int(st["waves"] - 1),
+                "requests": int(len(lat)), "span_s": span, "waves": int(st["waves"] - st0["waves"]),
                 "max_waves_in_flight": int(st["max_waves_in_flight"]),
                 "max_mem_in_use_bytes": int(st["max_mem_in_use"]), "launches": int(L.cmm_launch_count() - l0),
                 "clocks": clk}
 
     main_run = run(pool, True, arrivals)
+    # the same stream with every request hashing and planning for itself
+    no_cache = run(pool, True, arrivals, cache=0) if args.serve_cache_gb > 0 else None
     # latency without queueing: half the measured capacity, 10 s
     light_rate = 0.5 * main_run["products_per_s"]
     light = run(pool, True, np.cumsum(rng.exponential(1.0 / light_rate, size=int(light_rate * 10))))
@@ -504,11 +515,11 @@ def bench_serve(args, world, rank, local):
         return
     line = {
         "metric": METRIC, "value": main_run["products_per_s"], "unit": "products/s", "n_gpus": world,
-        "steps": main_run["requests"], "warmup": 8, "ms_per_step": 1e3 / main_run["products_per_s"],
+        "steps": main_run["requests"], "warmup": len(pool), "ms_per_step": 1e3 / main_run["products_per_s"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 (mixed: FP32 transforms, FP64 reduction)", "data": "synthetic", "config": config,
         "latency_ms": {"p50": main_run["p50_ms"], "p99": main_run["p99_ms"], "mean": main_run["mean_ms"]},
-        "serving": main_run, "unsaturated": light, "host_payload": host,
+        "serving": main_run, "serving_without_code_cache": no_cache, "unsaturated": light, "host_payload": host,
         "e2e": {"value": host["products_per_s"], "unit": "products/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": main_run["launches"], "clocks": main_run["clocks"], "roofline": None, "cpu_baseline": None,

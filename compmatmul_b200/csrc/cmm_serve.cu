@@ -28,6 +28,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <tuple>
 #include <vector>
 
 #include "cmm_batch.h"
@@ -64,6 +65,15 @@ class PinnedPool {
   std::map<size_t, std::vector<void*>> free_;
 };
 
+// hash codes and sorted plan of one (hash, seed, d, b, n_a, n_b, slab):
+// fixed by those alone, shared read-only by every request that has them
+struct CodePlan {
+  DevBuf params, codes_a, codes_b;
+  SlabPlan plan;
+  size_t bytes = 0;
+};
+using CodeKey = std::tuple<int, uint64_t, int, int, int64_t, int64_t, int>;
+
 struct Request {
   uint64_t id = 0;
   cmm_request r{};
@@ -73,8 +83,8 @@ struct Request {
   bool done = false;
   std::string error;
   // device state (allocated on the upload stream at admission)
-  DevBuf in_a, in_b, params, codes_a, codes_b, scale, partial, p_dev, work;
-  SlabPlan plan;
+  DevBuf in_a, in_b, scale, partial, p_dev, work;
+  std::shared_ptr<CodePlan> cp;  // codes + plan (cached or this request's own)
   SketchPlan sp{};
   const double2* tw = nullptr;
   cudaEvent_t prepared = nullptr;
@@ -122,6 +132,10 @@ struct Server {
   const double2* tw4096 = nullptr;
   PinnedPool pinned;
   std::thread th;
+  // residency of hash codes + plans (scheduler thread only), LRU order
+  std::map<CodeKey, std::pair<std::shared_ptr<CodePlan>, uint64_t>> cache;
+  uint64_t cache_clock = 0;
+  size_t cache_bytes = 0;
 };
 
 namespace {
@@ -195,21 +209,51 @@ void prepare(Server& S, Request& q) {
     AT = q.in_a.ptr;
     B = q.in_b.ptr;
   }
-  const SketchParams sp = make_sketch_params(r.hash_kind, r.d, r.b, r.seed);
-  q.params = DevBuf(sp.blob.size(), s);
-  CMM_CUDA(cudaMemcpyAsync(q.params.ptr, sp.blob.data(), sp.blob.size(), cudaMemcpyHostToDevice, s));
-  const size_t set = sp.fn_bytes * (size_t)r.d;
-  const uint8_t* base = q.params.as<uint8_t>();
-  q.codes_a = DevBuf(4 * (size_t)r.d * (size_t)std::max<int64_t>(r.n_a, 1), s);
-  q.codes_b = DevBuf(4 * (size_t)r.d * (size_t)std::max<int64_t>(r.n_b, 1), s);
-  launch_hash_codes(r.hash_kind, base, base + 2 * set, r.d, q.log2b, r.n_a, q.codes_a.as<uint32_t>(), s);
-  launch_hash_codes(r.hash_kind, base + set, base + 3 * set, r.d, q.log2b, r.n_b, q.codes_b.as<uint32_t>(), s);
+  // hash codes + sorted plan: from the residency cache, or built here
+  const CodeKey key{r.hash_kind, r.seed, r.d, r.b, r.n_a, r.n_b, q.logL};
+  auto hit = S.cache.find(key);
+  if (hit != S.cache.end()) {
+    q.cp = hit->second.first;
+    hit->second.second = ++S.cache_clock;
+    std::lock_guard<std::mutex> g(S.mu);
+    S.stats.cache_hits += 1;
+  } else {
+    auto cp = std::make_shared<CodePlan>();
+    const SketchParams sp = make_sketch_params(r.hash_kind, r.d, r.b, r.seed);
+    cp->params = DevBuf(sp.blob.size(), s);
+    CMM_CUDA(cudaMemcpyAsync(cp->params.ptr, sp.blob.data(), sp.blob.size(), cudaMemcpyHostToDevice, s));
+    const size_t set = sp.fn_bytes * (size_t)r.d;
+    const uint8_t* base = cp->params.as<uint8_t>();
+    cp->codes_a = DevBuf(4 * (size_t)r.d * (size_t)std::max<int64_t>(r.n_a, 1), s);
+    cp->codes_b = DevBuf(4 * (size_t)r.d * (size_t)std::max<int64_t>(r.n_b, 1), s);
+    launch_hash_codes(r.hash_kind, base, base + 2 * set, r.d, q.log2b, r.n_a, cp->codes_a.as<uint32_t>(), s);
+    launch_hash_codes(r.hash_kind, base + set, base + 3 * set, r.d, q.log2b, r.n_b, cp->codes_b.as<uint32_t>(), s);
+    cp->plan = make_residue_plan(cp->codes_a.as<uint32_t>(), cp->codes_b.as<uint32_t>(), r.n_a, r.n_b, r.d, r.b,
+                                 q.logL, 0, s);
+    cp->bytes = cp->params.bytes + cp->codes_a.bytes + cp->codes_b.bytes + cp->plan.srcA.bytes + cp->plan.srcB.bytes +
+                cp->plan.codeA.bytes + cp->plan.codeB.bytes + cp->plan.countA.bytes + cp->plan.countB.bytes;
+    q.cp = cp;
+    {
+      std::lock_guard<std::mutex> g(S.mu);
+      S.stats.cache_misses += 1;
+    }
+    if (S.cfg.cache_bytes > 0 && cp->bytes <= S.cfg.cache_bytes) {
+      while (S.cache_bytes + cp->bytes > S.cfg.cache_bytes && !S.cache.empty()) {  // evict least recent
+        auto lru = S.cache.begin();
+        for (auto it = S.cache.begin(); it != S.cache.end(); ++it)
+          if (it->second.second < lru->second.second) lru = it;
+        S.cache_bytes -= lru->second.first->bytes;
+        S.cache.erase(lru);  // in-flight requests keep their own reference
+      }
+      S.cache[key] = {cp, ++S.cache_clock};
+      S.cache_bytes += cp->bytes;
+    }
+  }
   q.scale = DevBuf(4 * (size_t)std::max<int64_t>(r.n_inner, 1), s);
   if (r.variant == kVariantFFT && r.n_inner > 0) {
     if (f32) launch_row_scale_f32((const float*)AT, (const float*)B, r.n_a, r.n_inner, r.n_b, q.scale.as<int>(), s);
     else launch_row_scale((const double*)AT, (const double*)B, r.n_a, r.n_inner, r.n_b, q.scale.as<int>(), s);
   }
-  q.plan = make_residue_plan(q.codes_a.as<uint32_t>(), q.codes_b.as<uint32_t>(), r.n_a, r.n_b, r.d, r.b, q.logL, 0, s);
   q.partial = DevBuf((size_t)q.G * r.d * (size_t)r.b * elem, s);
   CMM_CUDA(cudaMemsetAsync(q.partial.ptr, 0, q.partial.bytes, s));  // k-groups without rows stay zero
   q.p_dev = DevBuf((size_t)r.d * (size_t)r.b * 8, s);
@@ -226,15 +270,16 @@ BProd bprod(const Request& q) {
   BProd d{};
   d.AT = q.r.AT;
   d.B = q.r.B;
-  d.srcA = q.plan.srcA.as<uint32_t>();
-  d.srcB = q.plan.srcB.as<uint32_t>();
-  d.codeA = q.plan.codeA.ptr;
-  d.codeB = q.plan.codeB.ptr;
-  d.cutA = q.plan.countA.as<uint32_t>();
-  d.cutB = q.plan.countB.as<uint32_t>();
-  d.SA = q.plan.EA;
-  d.SB = q.plan.EB;
-  d.code16 = q.plan.u16 ? 1 : 0;
+  const SlabPlan& pl = q.cp->plan;
+  d.srcA = pl.srcA.as<uint32_t>();
+  d.srcB = pl.srcB.as<uint32_t>();
+  d.codeA = pl.codeA.ptr;
+  d.codeB = pl.codeB.ptr;
+  d.cutA = pl.countA.as<uint32_t>();
+  d.cutB = pl.countB.as<uint32_t>();
+  d.SA = pl.EA;
+  d.SB = pl.EB;
+  d.code16 = pl.u16 ? 1 : 0;
   d.scale = q.scale.as<int>();
   d.tw = q.tw;
   d.partial = q.partial.ptr;
@@ -326,14 +371,11 @@ void finish_wave(Server& S, std::unique_ptr<Wave>& W) {
     // device buffers return to the pool (their work has completed)
     q.in_a = DevBuf();
     q.in_b = DevBuf();
-    q.params = DevBuf();
-    q.codes_a = DevBuf();
-    q.codes_b = DevBuf();
     q.scale = DevBuf();
     q.partial = DevBuf();
     q.p_dev = DevBuf();
     q.work = DevBuf();
-    q.plan = SlabPlan();
+    q.cp.reset();  // a cached plan stays resident for later requests
     q.t_done = now;
   }
   S.pinned.put(W->host, W->host_cls);
@@ -442,6 +484,25 @@ Server* server_create(const cmm_server_config* cfg) {
   }
   S->ctas = batch_resident_ctas(cfg->f32 != 0);
   S->tw4096 = twiddles(1 << kBatchFftLog, S->up);
+  // map the admission cap into the stream-ordered pool once, so that
+  // admissions do not grow the pool while requests run (the pool keeps
+  // freed memory); less when the device has less free memory
+  {
+    { DevBuf first(256, S->up); }  // sets the pool to keep freed memory
+    size_t free_b = 0, total_b = 0;
+    CMM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    size_t want = std::min(cfg->mem_cap_bytes + cfg->cache_bytes, free_b / 10 * 9);
+    while (want >= ((size_t)64 << 20)) {
+      void* p = nullptr;
+      if (cudaMallocAsync(&p, want, S->up) == cudaSuccess) {
+        CMM_CUDA(cudaFreeAsync(p, S->up));
+        break;
+      }
+      cudaGetLastError();
+      want /= 2;
+    }
+    CMM_CUDA(cudaStreamSynchronize(S->up));
+  }
   S->th = std::thread(scheduler, S.get());
   return S.release();
 }
@@ -504,6 +565,7 @@ void server_stats(Server* S, cmm_server_stats* out) {
   *out = S->stats;
   out->mem_in_use = S->mem_in_use;
   out->max_mem_in_use = S->max_mem;
+  out->cache_in_use = S->cache_bytes;
 }
 
 void server_destroy(Server* S) {
@@ -519,6 +581,7 @@ void server_destroy(Server* S) {
     std::lock_guard<std::mutex> g(S->mu);
     err = S->error;
     S->by_id.clear();
+    S->cache.clear();
   }
   cudaStreamSynchronize(S->up);
   for (cudaStream_t s : S->streams) {

@@ -1,7 +1,7 @@
 """Serving engine (cmm_server_* of the C ABI): continuous batching of
 independent compressed products under a device-memory admission cap.
 
-    srv = Server(mem_cap_bytes=40 << 30, f32=True, streams=4, max_wave=32)
+    srv = Server(mem_cap_bytes=40 << 30, f32=True, streams=4, max_wave=32, cache_bytes=4 << 30)
     rid = srv.submit(AT, B, d, b, seed, variant="fft")   # returns at once
     p = srv.result(rid)                                    # waits; d x b float64
     srv.close()
@@ -21,7 +21,8 @@ from . import HASH_KINDS, VARIANTS, check, lib
 
 
 class _Config(C.Structure):
-    _fields_ = [("mem_cap_bytes", C.c_size_t), ("f32", C.c_int), ("streams", C.c_int), ("max_wave", C.c_int)]
+    _fields_ = [("mem_cap_bytes", C.c_size_t), ("f32", C.c_int), ("streams", C.c_int), ("max_wave", C.c_int),
+                ("cache_bytes", C.c_size_t)]
 
 
 class _Request(C.Structure):
@@ -33,7 +34,8 @@ class _Request(C.Structure):
 class _Stats(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("queued", C.c_int64),
                 ("in_flight", C.c_int64), ("waves", C.c_int64), ("max_waves_in_flight", C.c_int64),
-                ("mem_in_use", C.c_size_t), ("max_mem_in_use", C.c_size_t)]
+                ("mem_in_use", C.c_size_t), ("max_mem_in_use", C.c_size_t), ("cache_hits", C.c_int64),
+                ("cache_misses", C.c_int64), ("cache_in_use", C.c_size_t)]
 
 
 def _info(x, dtype):
@@ -51,10 +53,10 @@ def _info(x, dtype):
 
 
 class Server:
-    def __init__(self, mem_cap_bytes=40 << 30, f32=True, streams=4, max_wave=32):
+    def __init__(self, mem_cap_bytes=40 << 30, f32=True, streams=4, max_wave=32, cache_bytes=0):
         self.f32 = bool(f32)
         self._dtype = np.float32 if f32 else np.float64
-        cfg = _Config(int(mem_cap_bytes), int(self.f32), int(streams), int(max_wave))
+        cfg = _Config(int(mem_cap_bytes), int(self.f32), int(streams), int(max_wave), int(cache_bytes))
         h = C.c_void_p()
         check(lib().cmm_server_create(C.byref(cfg), C.byref(h)))
         self._h = h

@@ -265,6 +265,8 @@ typedef struct {
   int f32;               /* 1: float32 inputs (mixed precision); 0: float64 */
   int streams;           /* waves in flight at once (>= 1) */
   int max_wave;          /* most requests per wave (>= 1) */
+  size_t cache_bytes;    /* device bytes for hash codes + sorted plans kept across requests
+                            with the same (hash, seed, d, b, n_a, n_b); 0 disables the cache */
 } cmm_server_config;
 
 typedef struct {
@@ -281,6 +283,8 @@ typedef struct {
   int64_t submitted, completed, queued, in_flight;
   int64_t waves, max_waves_in_flight;
   size_t mem_in_use, max_mem_in_use;
+  int64_t cache_hits, cache_misses;
+  size_t cache_in_use;
 } cmm_server_stats;
 
 int cmm_server_create(const cmm_server_config* cfg, void** server);

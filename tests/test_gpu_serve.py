@@ -92,3 +92,25 @@ def test_serve_fp64_matches_oracle(gpu, oracle):
         ref = oracle.compressed_product(variant, hs, AT, B, d, b, seed)
         np.testing.assert_allclose(p, ref, rtol=0, atol=p_tol(ref, 1e-11))
     srv.close()
+
+
+@pytest.mark.gpu
+def test_serve_code_plan_cache(gpu):
+    """Requests with the same (hash, seed, d, b, sizes) share resident hash
+    codes and sorted plans: hits after the first, identical results."""
+    reqs = _requests(3, seed=53)
+    order = [0, 1, 2, 0, 1, 2, 2, 1, 0, 0]
+    plain = Server(mem_cap_bytes=4 << 30, f32=True, streams=2, max_wave=4)
+    want = [plain.result(plain.submit(q["AT"], q["B"], q["d"], q["b"], q["seed"], q["variant"])) for q in reqs]
+    plain.close()
+    srv = Server(mem_cap_bytes=4 << 30, f32=True, streams=2, max_wave=4, cache_bytes=1 << 30)
+    got = []
+    for k in order:  # one at a time: every repeat finds its entry resident
+        q = reqs[k]
+        got.append(srv.result(srv.submit(q["AT"], q["B"], q["d"], q["b"], q["seed"], q["variant"])))
+    st = srv.stats()
+    srv.close()
+    assert st["cache_misses"] == 3 and st["cache_hits"] == len(order) - 3, st
+    assert 0 < st["cache_in_use"] <= 1 << 30
+    for k, p in zip(order, got):
+        np.testing.assert_array_equal(p, want[k])
