@@ -171,10 +171,17 @@ static Codes make_codes(const SketchParams& sp, int64_t n_a, int64_t n_b, cudaSt
 }
 
 // Budget for the per-chunk materialized rows (d copies of each row pair).
+// Bytes for the materialized rows of one chunk of inner indices: a third of
+// the free device memory, at most 8 GiB, or CMM_MATERIALIZE_BYTES when set
+// (smaller budgets run more chunks).
 static size_t materialize_budget() {
   size_t free_b = 0, total_b = 0;
   CMM_CUDA(cudaMemGetInfo(&free_b, &total_b));
   size_t cap = (size_t)8 << 30;
+  if (const char* e = getenv("CMM_MATERIALIZE_BYTES")) {
+    const long long v = atoll(e);
+    if (v > 0 && (size_t)v < cap) cap = (size_t)v;
+  }
   return free_b / 3 < cap ? free_b / 3 : cap;
 }
 
@@ -210,7 +217,7 @@ static bool try_cluster_plan(int variant, bool f32, const Codes& codes, int64_t 
   }
   plan = make_residue_plan(codes.a.as<uint32_t>(), codes.b.as<uint32_t>(), n_a, n_b, sp.d, sp.b,
                            C.logL, C.logR2, s);
-  return cluster_smem_fits(variant, f32, plan);
+  return cluster_smem_fits(variant, f32, C, plan);
 }
 
 static void sketch_device(int variant, const SketchParams& sp, const Codes& codes, int64_t n_a,

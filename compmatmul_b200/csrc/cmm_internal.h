@@ -207,7 +207,7 @@ struct ClusterPlan {
 };
 bool sketch_cluster_applicable(int variant, bool f32, int b);
 ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, int64_t est_slots);
-bool cluster_smem_fits(int variant, bool f32, const SlabPlan& P);
+bool cluster_smem_fits(int variant, bool f32, const ClusterPlan& C, const SlabPlan& P);
 void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const SlabPlan& P,
                            const void* dMatA, const void* dMatB, int64_t kc, const int* dScaleExp,
                            int64_t k0, const double2* dTw, void* dPartial, int d, int accumulate,

@@ -26,6 +26,7 @@
 #include <cstdio>
 #include <cstdlib>
 
+#include "cmm_fft_device.cuh"
 #include "cmm_internal.h"
 
 namespace cg = cooperative_groups;
@@ -34,43 +35,10 @@ namespace cmm {
 namespace {
 
 constexpr int kCT = kPlanThreads;  // 512
-constexpr int kCBatch = 8;
+constexpr int kCBatch = 4;  // scatter slots loaded together
 constexpr int kCSkip = -0x7fffffff;
 
-// -------------------------------------------------------- complex helpers
-__device__ __forceinline__ double2 mk(double x, double y) { return make_double2(x, y); }
-__device__ __forceinline__ float2 mk(float x, float y) { return make_float2(x, y); }
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return mk(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
-}
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return mk(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
-}
-template <typename C>
-__device__ __forceinline__ void bf(C& a, C& b, C w) {
-  const C t = cmul(b, w);
-  b = mk(a.x - t.x, a.y - t.y);
-  a = mk(a.x + t.x, a.y + t.y);
-}
-template <typename C>
-__device__ __forceinline__ C csq(C a) {
-  return mk(a.x * a.x - a.y * a.y, (a.x + a.x) * a.y);
-}
-
-// three radix-2 DIT stages on x[0..7] (points base + e*half); W = w_{8half}^kk
-template <typename C>
-__device__ __forceinline__ void r8(C (&x)[8], C W) {
-  using R = decltype(W.x);
-  const R h = (R)0.70710678118654752440;
-  const C W2 = csq(W), W4 = csq(W2);
-  bf(x[0], x[1], W4); bf(x[2], x[3], W4); bf(x[4], x[5], W4); bf(x[6], x[7], W4);
-  const C W2m = mk(W2.y, -W2.x);
-  bf(x[0], x[2], W2); bf(x[4], x[6], W2); bf(x[1], x[3], W2m); bf(x[5], x[7], W2m);
-  const C W1 = cmul(W, mk(h, -h));
-  const C Wi = mk(W.y, -W.x);
-  const C W3 = cmul(W, mk(-h, -h));
-  bf(x[0], x[4], W); bf(x[1], x[5], W1); bf(x[2], x[6], Wi); bf(x[3], x[7], W3);
-}
+using namespace dev;
 
 // DFT_8 with natural-order input and output
 template <typename C>
@@ -82,34 +50,17 @@ __device__ __forceinline__ void dft8(C (&u)[8]) {
   for (int e = 0; e < 8; ++e) u[e] = x[e];
 }
 
-template <typename R, int M>
-__device__ __forceinline__ void whtr(R (&x)[M]) {
-#pragma unroll
-  for (int h = 1; h < M; h <<= 1)
-#pragma unroll
-    for (int e = 0; e < M; ++e)
-      if (!(e & h)) {
-        const R a = x[e], b = x[e + h];
-        x[e] = a + b;
-        x[e + h] = a - b;
-      }
-}
-
-__device__ __forceinline__ void tsum(float& hi, float& lo, float x) {
-  const float s = hi + x;
-  const float bp = s - hi;
-  lo += (hi - (s - bp)) + (x - bp);
-  hi = s;
-}
-
-// padded shared layouts: 16-byte elements p + p/8, 8-byte p + p/16, 4-byte p + p/32
+// padded shared layouts: 16- and 8-byte elements p + p/16, 4-byte p + p/32.
+// One spare element per 16 keeps the radix passes conflict-free and spreads
+// the scatter's bit-reversed positions (a warp's buckets differ in bits that
+// land in p/16) over all banks.
 template <int ES>
 __device__ __forceinline__ int phys(int p) {
-  return ES == 16 ? p + (p >> 3) : (ES == 8 ? p + (p >> 4) : p + (p >> 5));
+  return ES == 4 ? p + (p >> 5) : p + (p >> 4);
 }
 template <int ES>
 constexpr int phys_len(int L) {
-  return ES == 16 ? L + L / 8 : (ES == 8 ? L + L / 16 : L + L / 32);
+  return ES == 4 ? L + L / 32 : L + L / 16;
 }
 
 // ------------------------------------------------- tensor-core H16 (FP32)
@@ -168,7 +119,7 @@ struct ClArgs {
   const void* matB;
   const void* codeA;  // [t][R2][SA]
   const void* codeB;
-  const uint32_t* countA;  // [t][R2][512]
+  const uint32_t* countA;  // [t][R2][513] cut offsets
   const uint32_t* countB;
   const int* scale_exp;
   const double2* tw;  // w_b^j
@@ -177,8 +128,69 @@ struct ClArgs {
   int d, log2b, logR1, logR2, G, accumulate;
 };
 
-// VARIANT 0 = FFT, 1 = FWHT; Real = double (plain) or float (mixed)
-template <int VARIANT, typename Real, typename CodeT>
+// Staged slot e of a segment sits at e + e / 16 (8-byte values) or e + e / 8
+// (4-byte values): neighbouring threads' ranges start a few slots apart, and
+// the spare slots spread their same-index reads over the banks.
+__host__ __device__ constexpr int64_t spad_len_n(int64_t n, size_t real) {
+  return n + n / (real == 8 ? 16 : 8) + 1;
+}
+template <typename Real>
+__device__ __forceinline__ int spad(int e) { return e + (e >> (sizeof(Real) == 8 ? 4 : 3)); }
+template <typename Real>
+__device__ __forceinline__ int64_t spad_len(int64_t n) { return spad_len_n(n, sizeof(Real)); }
+
+// entries of the coarse DIF weight table w_b^{512 j}, j < b / 512
+__host__ __device__ inline int cl_pre_hi(int log2b) { return log2b > 9 ? 1 << (log2b - 9) : 1; }
+
+// Shared-memory layout of one CTA, shared by the kernel and the host sizing:
+// NB sub-spectrum buffers, then (FFT) the factored post-twiddle tables, the
+// DIF weight tables when R1 > 1, the pass twiddles and w_R1; then the staged
+// row values of this CTA's segments and their premixed codes.
+struct ClLayout {
+  size_t buf, post, pre, ptw, wr, stage, codes, total;
+};
+__host__ __device__ inline size_t cl_align16(size_t x) { return (x + 15) & ~(size_t)15; }
+__host__ __device__ inline ClLayout cl_layout(bool fft, bool f32, bool u16, int NB, int R1, int log2b,
+                                              int64_t SA, int64_t SB) {
+  const size_t real = f32 ? 4 : 8, cpx = 2 * real;
+  const size_t L = (fft && !f32) ? 4096 : 8192;
+  auto plen = [](size_t n, size_t es) { return es == 4 ? n + n / 32 : n + n / 16; };
+  ClLayout o;
+  size_t p = 0;
+  o.buf = p;
+  p += (size_t)NB * (fft ? plen(L, cpx) * cpx : 2 * plen(L, real) * real);
+  o.post = p;
+  if (fft) p += (128 + 64) * cpx;
+  o.pre = p;
+  if (fft && R1 > 1) p += (cl_pre_hi(log2b) + 512) * cpx;
+  o.ptw = p;
+  if (fft) p += (f32 ? 1176 : 592) * cpx;
+  o.wr = p;
+  p += 32 * real;
+  o.stage = p;
+  p += cl_align16((size_t)(spad_len_n(SA, real) + spad_len_n(SB, real)) * real);
+  o.codes = p;
+  p += cl_align16((size_t)(SA + SB) * (u16 ? 2 : 4));
+  o.total = p;
+  return o;
+}
+
+static __device__ __forceinline__ void cp_async4(void* sdst, const void* gsrc) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((uint32_t)__cvta_generic_to_shared(sdst)),
+               "l"(gsrc)
+               : "memory");
+}
+static __device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((uint32_t)__cvta_generic_to_shared(sdst)),
+               "l"(gsrc)
+               : "memory");
+}
+static __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// VARIANT 0 = FFT, 1 = FWHT; Real = double (plain) or float (mixed); NB = 2
+// double-buffers the sub-spectra (one cluster barrier per inner index), NB = 1
+// when two buffers do not fit in shared memory (two barriers).
+template <int VARIANT, typename Real, typename CodeT, int NB>
 __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
   constexpr bool kFFT = VARIANT == kVariantFFT;
   constexpr bool kF32 = sizeof(Real) == 4;
@@ -197,34 +209,33 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
   const int logM = a.log2b - a.logR1;  // M = b / R1
   const double2* tw = a.tw;
 
-  // ---- shared layout
-  unsigned char* p = sm;
-  C* buf = nullptr;     // FFT: L complex
-  Real* xs = nullptr;   // FWHT: L real (A side)
-  Real* ys = nullptr;   // FWHT: L real (B side)
-  if (kFFT) { buf = reinterpret_cast<C*>(p); p += PL * sizeof(C); }
-  else { xs = reinterpret_cast<Real*>(p); ys = xs + PL; p += 2 * PL * sizeof(Real); }
-  C* post = reinterpret_cast<C*>(p);            // FFT: w_M^{n r2}, n < L
-  if (kFFT) p += L * sizeof(C);
-  C* preHi = reinterpret_cast<C*>(p);           // FFT, R1 > 1: w_b^{x}, x = hi * 512 + lo
-  C* preLo = preHi + 1024;
-  if (kFFT) p += (1024 + 512) * sizeof(C);
-  C* ptw = reinterpret_cast<C*>(p);             // FFT pass twiddles (<= 1176)
-  if (kFFT) p += 1184 * sizeof(C);
-  Real* wRx = reinterpret_cast<Real*>(p);       // FFT: Re/Im w_R1^j, j < 16
+  // ---- shared layout (cl_layout)
+  const ClLayout lay = cl_layout(kFFT, kF32, sizeof(CodeT) == 2, NB, R1, a.log2b, a.SA, a.SB);
+  C* buf0 = reinterpret_cast<C*>(sm + lay.buf);        // FFT: NB x PL complex
+  Real* xs0 = reinterpret_cast<Real*>(sm + lay.buf);   // FWHT: NB x (x: PL, y: PL) real
+  C* postLo = reinterpret_cast<C*>(sm + lay.post);     // FFT: w_M^{n r2} = postHi[n >> 7] postLo[n & 127]
+  C* postHi = postLo + 128;
+  C* preHi = reinterpret_cast<C*>(sm + lay.pre);       // FFT, R1 > 1: w_b^{x}, x = hi * 512 + lo
+  C* preLo = preHi + cl_pre_hi(a.log2b);
+  C* ptw = reinterpret_cast<C*>(sm + lay.ptw);         // FFT pass twiddles (592 FP64, 1176 FP32)
+  Real* wRx = reinterpret_cast<Real*>(sm + lay.wr);    // FFT: Re/Im w_R1^j, j < 16
   Real* wRy = wRx + 16;
-  p += 32 * sizeof(Real);
-  CodeT* cA = reinterpret_cast<CodeT*>(p);
+  Real* stA = reinterpret_cast<Real*>(sm + lay.stage);  // staged row values, this CTA's segments
+  Real* stB = stA + spad_len<Real>(a.SA);
+  CodeT* cA = reinterpret_cast<CodeT*>(sm + lay.codes);
   CodeT* cB = cA + a.SA;
 
   // ---- tables (constant over k)
   if (kFFT) {
-    for (int n = tid; n < L; n += kCT) {
-      const double2 w = tw[((uint64_t)n * (uint64_t)r2) << a.logR1];  // w_M^{n r2} = w_b^{n r2 R1}
-      post[n] = mk((Real)w.x, (Real)w.y);
+    for (int e = tid; e < 128 + 64; e += kCT) {
+      const uint64_t n = e < 128 ? (uint64_t)e : (uint64_t)(e - 128) << 7;
+      if (n < (uint64_t)L) {
+        const double2 w = tw[(n * (uint64_t)r2) << a.logR1];  // w_M^{n r2} = w_b^{n r2 R1}
+        postLo[e] = mk((Real)w.x, (Real)w.y);
+      }
     }
     if (R1 > 1) {
-      for (int e = tid; e < 1024; e += kCT) {
+      for (int e = tid; e < cl_pre_hi(a.log2b); e += kCT) {
         const uint64_t x = (uint64_t)e << 9;
         const double2 w = x < ((uint64_t)1 << a.log2b) ? tw[x] : make_double2(1.0, 0.0);
         preHi[e] = mk((Real)w.x, (Real)w.y);
@@ -261,6 +272,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
       wRy[e] = (Real)w.y;
     }
   }
+  auto post = [&](int n) -> C { return cmul(postHi[n >> 7], postLo[n & 127]); };
   // B fragments of H16 for the FP32 FWHT
   uint32_t hb[2][2] = {{0u, 0u}, {0u, 0u}};
   if (!kFFT && kF32) {
@@ -274,6 +286,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
     }
   }
 
+  unsigned step = 0;  // inner indices processed by this CTA (selects the buffer)
   // ---- persistent loop over work items (r1, t, k-group); every CTA of a
   // cluster has the same blockIdx.y, hence the same items and barriers
   const int items = (R1 * a.d) * a.G;
@@ -281,7 +294,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
   const int r1 = item & (R1 - 1);
   const int t = (item >> a.logR1) % a.d;
   const int g = (item >> a.logR1) / a.d;
-  __syncthreads();  // the previous item is done with the shared codes
+  __syncthreads();  // the previous item is done with the shared codes and staged rows
   // codes of this CTA's segment, premixed with the DIF weight index for r1
   {
     const CodeT* gA = reinterpret_cast<const CodeT*>(a.codeA) + ((size_t)t * R2 + r2) * a.SA;
@@ -341,80 +354,132 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
   const int64_t per = (a.kc + a.G - 1) / a.G;
   const int64_t kb = (int64_t)g * per;
   const int64_t ke = kb + per < a.kc ? kb + per : a.kc;
-  cluster.sync();
+  // the next inner index with a nonzero row pair (all-zero rows are skipped
+  // identically by every CTA of the cluster)
+  auto next_k = [&](int64_t k) -> int64_t {
+    if (kFFT)
+      while (k < ke && __ldg(a.scale_exp + a.k0 + k) == kCSkip) ++k;
+    return k;
+  };
+  // stage this CTA's segments of row k, coalesced (thread i copies slots i,
+  // i + 512, ...); the copies land before the barrier that precedes the
+  // scatter, and are issued after the barrier that ends the previous scatter
+  const int totA = (int)cutA[kCT], totB = (int)cutB[kCT];
+  auto stage = [&](int64_t k) {
+    const Real* rA = reinterpret_cast<const Real*>(a.matA) + (((size_t)t * a.kc + k) * R2 + r2) * a.SA;
+    const Real* rB = reinterpret_cast<const Real*>(a.matB) + (((size_t)t * a.kc + k) * R2 + r2) * a.SB;
+    for (int e = tid; e < totA; e += kCT) {
+      if (kF32) cp_async4(stA + spad<Real>(e), rA + e); else cp_async8(stA + spad<Real>(e), rA + e);
+    }
+    for (int e = tid; e < totB; e += kCT) {
+      if (kF32) cp_async4(stB + spad<Real>(e), rB + e); else cp_async8(stB + spad<Real>(e), rB + e);
+    }
+  };
+  int64_t kk = next_k(kb);
+  if (kk < ke) stage(kk);
+  cluster.sync();  // tables and codes written; the previous item's reads are done
 
-  for (int64_t kk = kb; kk < ke; ++kk) {
+  while (kk < ke) {
+    const int64_t kn = next_k(kk + 1);
     Real alpha = (Real)1, beta = (Real)1;
     if (kFFT) {
       const int se = __ldg(a.scale_exp + a.k0 + kk);
-      if (se == kCSkip) continue;  // the same for every CTA of the cluster
       alpha = kF32 ? (Real)__int_as_float((127 - se) << 23) : (Real)__longlong_as_double((long long)(1023 - se) << 52);
       beta = kF32 ? (Real)__int_as_float((127 + se) << 23) : (Real)__longlong_as_double((long long)(1023 + se) << 52);
+    }
+    C* buf = buf0 + (NB == 2 ? (size_t)(step & 1) * PL : 0);
+    Real* xs = xs0 + (NB == 2 ? (size_t)(step & 1) * 2 * PL : 0);
+    Real* ys = xs + PL;
+    if (kFFT) {
       for (int e = tid; e < PL; e += kCT) buf[e] = mk((Real)0, (Real)0);
     } else {
       for (int e = tid; e < PL; e += kCT) { xs[e] = (Real)0; ys[e] = (Real)0; }
     }
+    cp_async_wait_all();  // this thread's copies of row kk; the barrier publishes all
     __syncthreads();
-    // ---- scatter this CTA's residue segment (run accumulation, one store per bucket)
+    // ---- scatter this CTA's residue segment.  The plan cuts the segment at
+    // bucket boundaries, so every bucket has one writer thread; its slots are
+    // sorted by bucket.  Per batch of kCBatch slots a thread loads every
+    // target first, sums runs of equal buckets in registers and stores once
+    // per run.  The scale is a power of two, applied per value.  Side A and
+    // side B write different words when the DIF weights are real (FFT with
+    // R1 <= 2: real / imaginary part; FWHT: x / y), so both sides run at once.
+    const bool split = !kFFT || R1 <= 2;
 #pragma unroll
     for (int side = 0; side < 2; ++side) {
-      const Real* row = reinterpret_cast<const Real*>(side == 0 ? a.matA : a.matB) +
-                        (((size_t)t * a.kc + kk) * R2 + r2) * (side == 0 ? a.SA : a.SB);
+      const Real* st = side == 0 ? stA : stB;
       const CodeT* codes = side == 0 ? cA : cB;
       const int beg = side == 0 ? begA : begB, end = side == 0 ? endA : endB;
       const Real sc = side == 0 ? alpha : beta;
-      uint32_t cur = 0xffffffffu;
-      C acc = mk((Real)0, (Real)0);
-      auto flush = [&](uint32_t m) {
-        if (kFFT) {
-          const uint32_t pos = __brev(m) >> (32 - LOGL);
-          C& dst = buf[phys<ES>((int)pos)];
-          if (side == 0) dst = mk(acc.x * sc, acc.y * sc);
-          else dst = mk(fma(acc.x, sc, dst.x), fma(acc.y, sc, dst.y));
-        } else {
-          (side == 0 ? xs : ys)[phys<ES>((int)m)] = acc.x;
-        }
-      };
+      Real* words = kFFT ? reinterpret_cast<Real*>(buf) + side : (side == 0 ? xs : ys);
+      constexpr int kWordStride = kFFT ? 2 : 1;  // Real words per element
       for (int s0 = beg; s0 < end; s0 += kCBatch) {
-        Real vv[kCBatch];
-        uint32_t hh[kCBatch];
+        Real cx[kCBatch], cy[kCBatch];
+        int pp[kCBatch];
+        uint32_t mm[kCBatch];
 #pragma unroll
         for (int u = 0; u < kCBatch; ++u) {
-          const bool ok = s0 + u < end;
           const int e = s0 + u;
-          vv[u] = ok ? __ldg(row + e) : (Real)0;
-          hh[u] = ok ? (uint32_t)codes[e] : 0xffffffffu;
-        }
-#pragma unroll
-        for (int u = 0; u < kCBatch; ++u) {
-          if (hh[u] == 0xffffffffu) break;
-          const uint32_t h = hh[u];
+          const bool ok = e < end;
+          const Real v = ok ? st[spad<Real>(e)] * sc : (Real)0;
+          const uint32_t h = ok ? (uint32_t)codes[e] : 0u;
           const uint32_t m = h & (L - 1), w = h >> LOGL;
-          C c;
-          if (kFFT) {
-            const Real wx = wRx[w], wy = wRy[w];
-            c = side == 0 ? mk(vv[u] * wx, vv[u] * wy) : mk(-vv[u] * wy, vv[u] * wx);
+          mm[u] = ok ? m : 0xffffffffu;
+          pp[u] = phys<ES>(kFFT ? (int)(__brev(m) >> (32 - LOGL)) : (int)m);
+          if (!kFFT) {
+            cx[u] = w ? -v : v;
+            cy[u] = (Real)0;
+          } else if (split) {
+            cx[u] = (w & 1u) ? -v : v;  // w_2^w = +-1 (w = 0 when R1 = 1)
+            cy[u] = (Real)0;
+          } else if (a.logR1 == 2) {  // w_4^w = (-i)^w exactly
+            cx[u] = (w & 1u) ? (Real)0 : ((w & 2u) ? -v : v);
+            cy[u] = (w & 1u) ? ((w & 2u) ? v : -v) : (Real)0;
           } else {
-            c = mk(w ? -vv[u] : vv[u], (Real)0);
+            cx[u] = v * wRx[w];
+            cy[u] = v * wRy[w];
           }
-          if (m != cur) {
-            if (cur != 0xffffffffu) flush(cur);
-            cur = m;
-            acc = c;
-          } else {
-            acc.x += c.x;
-            acc.y += c.y;
+          if (kFFT && !split && side == 1) {  // side B adds i c
+            const Real tx = cx[u];
+            cx[u] = -cy[u];
+            cy[u] = tx;
+          }
+        }
+        if (split) {
+          Real old[kCBatch];
+#pragma unroll
+          for (int u = 0; u < kCBatch; ++u) old[u] = mm[u] != 0xffffffffu ? words[pp[u] * kWordStride] : (Real)0;
+          Real rx = (Real)0;
+#pragma unroll
+          for (int u = 0; u < kCBatch; ++u) {
+            rx = (u > 0 && mm[u] == mm[u - 1]) ? rx + cx[u] : cx[u];
+            const bool last = u == kCBatch - 1 || mm[u + 1] != mm[u];
+            if (mm[u] != 0xffffffffu && last) words[pp[u] * kWordStride] = old[u] + rx;
+          }
+        } else {
+          C old[kCBatch];
+#pragma unroll
+          for (int u = 0; u < kCBatch; ++u) old[u] = mm[u] != 0xffffffffu ? buf[pp[u]] : mk((Real)0, (Real)0);
+          Real rx = (Real)0, ry = (Real)0;
+#pragma unroll
+          for (int u = 0; u < kCBatch; ++u) {
+            const bool cont = u > 0 && mm[u] == mm[u - 1];
+            rx = cont ? rx + cx[u] : cx[u];
+            ry = cont ? ry + cy[u] : cy[u];
+            const bool last = u == kCBatch - 1 || mm[u + 1] != mm[u];
+            if (mm[u] != 0xffffffffu && last) buf[pp[u]] = mk(old[u].x + rx, old[u].y + ry);
           }
         }
       }
-      if (cur != 0xffffffffu) flush(cur);
-      if (kFFT) __syncthreads();
+      if (side == 0 && !split) __syncthreads();
     }
-    if (!kFFT) __syncthreads();
+    __syncthreads();         // the scatter is done with the staged row
+    if (kn < ke) stage(kn);  // overlaps the transform and the combine
 
     // ---- local transform of length L (results stay in shared memory)
     if (kFFT && !kF32) {
-      // 4 radix-8 DIT passes; pass 0 applies the DIF twiddle w_b^{n1 r1}
+      // 4 radix-8 DIT passes; pass 0 (constant twiddles) applies the DIF
+      // weight w_b^{n1 r1}, pass 3 the post-twiddle w_M^{n r2}
 #pragma unroll
       for (int ps = 0; ps < 4; ++ps) {
         const int s0 = 3 * ps, half = 1 << s0;
@@ -423,22 +488,26 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
         C x[8];
 #pragma unroll
         for (int e = 0; e < 8; ++e) x[e] = buf[phys<ES>(base + e * half)];
-        if (ps == 0 && R1 > 1) {
+        if (ps == 0) {
+          if (R1 > 1) {
 #pragma unroll
-          for (int e = 0; e < 8; ++e) {
-            const uint32_t m = __brev((uint32_t)(base + e)) >> (32 - LOGL);
-            const uint32_t xx = ((m << a.logR2) + (uint32_t)r2) * (uint32_t)r1;  // n1 r1 < b
-            x[e] = cmul(x[e], cmul(preHi[xx >> 9], preLo[xx & 511]));
+            for (int e = 0; e < 8; ++e) {
+              const uint32_t m = __brev((uint32_t)(base + e)) >> (32 - LOGL);
+              const uint32_t xx = ((m << a.logR2) + (uint32_t)r2) * (uint32_t)r1;  // n1 r1 < b
+              x[e] = cmul(x[e], cmul(preHi[xx >> 9], preLo[xx & 511]));
+            }
           }
+          r8_first(x);
+        } else {
+          r8(x, ptw[(ps == 1 ? 0 : (ps == 2 ? 8 : 72)) + kk2]);
         }
-        r8(x, ps == 0 ? mk((Real)1, (Real)0) : ptw[(ps == 1 ? 0 : (ps == 2 ? 8 : 72)) + kk2]);
         if (ps == 3) {
 #pragma unroll
-          for (int e = 0; e < 8; ++e) x[e] = cmul(x[e], post[base + e * half]);
+          for (int e = 0; e < 8; ++e) x[e] = cmul(x[e], post(base + e * half));
         }
 #pragma unroll
         for (int e = 0; e < 8; ++e) buf[phys<ES>(base + e * half)] = x[e];
-        __syncthreads();
+        if (ps < 3) __syncthreads();
       }
     } else if (kFFT) {
       // FP32, L = 8192: radix-16 (stages 0-3) + 3 radix-8 passes
@@ -455,8 +524,17 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
             x[e] = cmul(x[e], cmul(preHi[xx >> 9], preLo[xx & 511]));
           }
         }
+        // stages 0 and 1 have the twiddles 1 and -i
 #pragma unroll
-        for (int st = 0; st < 4; ++st) {
+        for (int e = 0; e < 16; e += 2) add_sub(x[e], x[e + 1]);
+#pragma unroll
+        for (int e = 0; e < 16; e += 4) {
+          add_sub(x[e], x[e + 2]);
+          x[e + 3] = mul_mi(x[e + 3]);
+          add_sub(x[e + 1], x[e + 3]);
+        }
+#pragma unroll
+        for (int st = 2; st < 4; ++st) {
           const int hh = 1 << st;
 #pragma unroll
           for (int e = 0; e < 16; ++e) {
@@ -482,12 +560,12 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
           r8(x, ptw[(ps == 1 ? 0 : (ps == 2 ? 16 : 144)) + kk2]);
           if (ps == 3) {
 #pragma unroll
-            for (int e = 0; e < 8; ++e) x[e] = cmul(x[e], post[base + e * half]);
+            for (int e = 0; e < 8; ++e) x[e] = cmul(x[e], post(base + e * half));
           }
 #pragma unroll
           for (int e = 0; e < 8; ++e) buf[phys<ES>(base + e * half)] = x[e];
         }
-        __syncthreads();
+        if (ps < 3) __syncthreads();
       }
     } else if (!kF32) {
       // FP64 WHT of x and y: radix-16 + 3 radix-8 passes, natural order
@@ -517,7 +595,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
 #pragma unroll
           for (int e = 0; e < 8; ++e) { xs[phys<ES>(base + e * half)] = x[e]; ys[phys<ES>(base + e * half)] = y[e]; }
         }
-        __syncthreads();
+        if (ps < 3) __syncthreads();
       }
     } else {
       // FP32 WHT: three Hadamard-16 factors on the tensor cores + radix-2
@@ -540,12 +618,13 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
         fx[phys<ES>(m)] = x0 + x1; fx[phys<ES>(m + 4096)] = x0 - x1;
         fy[phys<ES>(m)] = y0 + y1; fy[phys<ES>(m + 4096)] = y0 - y1;
       }
-      __syncthreads();
     }
 
     cluster.sync();  // every sub-spectrum of the cluster is complete
 
-    // ---- radix-R2 combine across the cluster; accumulate
+    // ---- radix-R2 combine across the cluster; accumulate.  With R2 = 16 the
+    // two threads of a lane pair own the even / odd outputs of one position:
+    // each reads half of the 16 sub-spectra and they swap halves by shuffle.
 #pragma unroll
     for (int u = 0; u < OUT / 8; ++u) {
       const int gi = tid + kCT * u;
@@ -555,14 +634,15 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
       if (kFFT) {
         C z[8];
         if (R2 == 16) {
+          const int rb = half ? 8 : 0;
+#pragma unroll
+          for (int r = 0; r < 8; ++r) z[r] = cluster.map_shared_rank(buf, rb + r)[phys<ES>(n)];
 #pragma unroll
           for (int r = 0; r < 8; ++r) {
-            const C* b0 = cluster.map_shared_rank(buf, r);
-            const C* b8 = cluster.map_shared_rank(buf, r + 8);
-            const C lo = b0[phys<ES>(n)], hi = b8[phys<ES>(n)];
+            const C o = mk(__shfl_xor_sync(0xffffffffu, z[r].x, 1), __shfl_xor_sync(0xffffffffu, z[r].y, 1));
             // even outputs: z_r + z_{r+8}; odd outputs: w_16^r (z_r - z_{r+8})
-            if (half == 0) z[r] = mk(lo.x + hi.x, lo.y + hi.y);
-            else z[r] = cmul(mk(lo.x - hi.x, lo.y - hi.y), ptw[(kF32 ? 1168 : 584) + r]);
+            if (half == 0) z[r] = mk(z[r].x + o.x, z[r].y + o.y);
+            else z[r] = cmul(mk(o.x - z[r].x, o.y - z[r].y), ptw[(kF32 ? 1168 : 584) + r]);
           }
         } else {
 #pragma unroll
@@ -585,16 +665,17 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
       } else {
         Real zx[8], zy[8];
         if (R2 == 16) {
+          const int rb = half ? 8 : 0;
 #pragma unroll
           for (int r = 0; r < 8; ++r) {
-            const Real* x0 = cluster.map_shared_rank(xs, r);
-            const Real* x8 = cluster.map_shared_rank(xs, r + 8);
-            const Real* y0 = cluster.map_shared_rank(ys, r);
-            const Real* y8 = cluster.map_shared_rank(ys, r + 8);
-            const Real a0 = x0[phys<ES>(n)], a8 = x8[phys<ES>(n)];
-            const Real c0 = y0[phys<ES>(n)], c8 = y8[phys<ES>(n)];
-            zx[r] = half == 0 ? a0 + a8 : a0 - a8;
-            zy[r] = half == 0 ? c0 + c8 : c0 - c8;
+            zx[r] = cluster.map_shared_rank(xs, rb + r)[phys<ES>(n)];
+            zy[r] = cluster.map_shared_rank(ys, rb + r)[phys<ES>(n)];
+          }
+#pragma unroll
+          for (int r = 0; r < 8; ++r) {
+            const Real ox = __shfl_xor_sync(0xffffffffu, zx[r], 1), oy = __shfl_xor_sync(0xffffffffu, zy[r], 1);
+            zx[r] = half == 0 ? zx[r] + ox : ox - zx[r];
+            zy[r] = half == 0 ? zy[r] + oy : oy - zy[r];
           }
         } else {
 #pragma unroll
@@ -613,7 +694,9 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
         }
       }
     }
-    cluster.sync();  // all reads of the sub-spectra are done
+    if (NB == 1) cluster.sync();  // all reads of the sub-spectra are done
+    ++step;
+    kk = kn;
   }
 
 #pragma unroll
@@ -626,6 +709,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
     else partR[f] = vx;
   }
   }  // item loop
+  if (NB == 2) cluster.sync();  // the other CTAs' last reads of this CTA's buffers
 }
 
 // ------------------------------------------------------------------ host
@@ -638,29 +722,29 @@ bool sketch_cluster_applicable(int variant, bool f32, int b) {
   return log2b - logL >= 3 && log2b <= 19;  // R >= 8; DIF twiddle table covers b <= 2^19
 }
 
-template <int V, typename Real, typename CodeT>
+constexpr size_t kClSmemMax = 227 * 1024;
+
+template <int V, typename Real, typename CodeT, int NB>
 static void cl_kernel_attrs(size_t smem) {
-  CMM_CUDA(cudaFuncSetAttribute(k_sketch_cluster<V, Real, CodeT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  CMM_CUDA(cudaFuncSetAttribute(k_sketch_cluster<V, Real, CodeT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  auto k = k_sketch_cluster<V, Real, CodeT, NB>;
+  CMM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CMM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
 }
 
-static size_t cl_smem(int variant, bool f32, bool u16, int64_t SA, int64_t SB) {
-  const int L = 1 << cl_logL(variant, f32);
-  const size_t real = f32 ? 4 : 8, cpx = 2 * real;
-  size_t s;
-  if (variant == kVariantFFT) {
-    const size_t pl = f32 ? (size_t)L + L / 16 : (size_t)L + L / 8;
-    s = pl * cpx + (size_t)L * cpx + (1024 + 512) * cpx + 1184 * cpx;
-  } else {
-    const size_t pl = f32 ? (size_t)L + L / 32 : (size_t)L + L / 16;
-    s = 2 * pl * real;
+// shared bytes of one CTA and the buffer count: two sub-spectrum buffers
+// when they fit, else one
+static size_t cl_smem(int variant, bool f32, bool u16, int R1, int log2b, int64_t SA, int64_t SB, int* nb) {
+  const bool fft = variant == kVariantFFT;
+  const size_t two = cl_layout(fft, f32, u16, 2, R1, log2b, SA, SB).total;
+  if (two <= kClSmemMax) {
+    if (nb) *nb = 2;
+    return two;
   }
-  s += 32 * real;
-  s += (size_t)(SA + SB) * (u16 ? 2 : 4);
-  return s;
+  if (nb) *nb = 1;
+  return cl_layout(fft, f32, u16, 1, R1, log2b, SA, SB).total;
 }
 
-template <int V, typename Real, typename CodeT>
+template <int V, typename Real, typename CodeT, int NB>
 static void cl_launch(const ClArgs& a, dim3 grid, int R2, size_t smem, cudaStream_t s) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
@@ -674,12 +758,12 @@ static void cl_launch(const ClArgs& a, dim3 grid, int R2, size_t smem, cudaStrea
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  CMM_CUDA(cudaLaunchKernelEx(&cfg, k_sketch_cluster<V, Real, CodeT>, a));
+  CMM_CUDA(cudaLaunchKernelEx(&cfg, k_sketch_cluster<V, Real, CodeT, NB>, a));
 }
 
 template <int V, typename Real, typename CodeT>
 static int cl_max_clusters(int R2, size_t smem) {
-  cl_kernel_attrs<V, Real, CodeT>(smem);
+  cl_kernel_attrs<V, Real, CodeT, 1>(smem);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)R2, 1, 1);
   cfg.blockDim = dim3(kCT, 1, 1);
@@ -692,7 +776,7 @@ static int cl_max_clusters(int R2, size_t smem) {
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   int n = 0;
-  if (cudaOccupancyMaxActiveClusters(&n, k_sketch_cluster<V, Real, CodeT>, &cfg) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveClusters(&n, k_sketch_cluster<V, Real, CodeT, 1>, &cfg) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
@@ -713,7 +797,7 @@ ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, i
   for (int logR2 : {4, 3}) {
     if (logR2 > logR) continue;
     const int R2 = 1 << logR2, R1 = 1 << (logR - logR2);
-    const size_t smem = cl_smem(variant, f32, true, est_slots, est_slots);
+    const size_t smem = cl_smem(variant, f32, true, R1, C.log2b, est_slots, est_slots, nullptr);
     int mx;
     if (variant == kVariantFFT)
       mx = f32 ? cl_max_clusters<0, float, uint16_t>(R2, smem) : cl_max_clusters<0, double, uint16_t>(R2, smem);
@@ -744,8 +828,8 @@ ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, i
   return C;
 }
 
-bool cluster_smem_fits(int variant, bool f32, const SlabPlan& P) {
-  return cl_smem(variant, f32, P.u16, P.EA, P.EB) <= 227 * 1024;
+bool cluster_smem_fits(int variant, bool f32, const ClusterPlan& C, const SlabPlan& P) {
+  return cl_smem(variant, f32, P.u16, 1 << C.logR1, C.log2b, P.EA, P.EB, nullptr) <= kClSmemMax;
 }
 
 void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const SlabPlan& P,
@@ -773,16 +857,24 @@ void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const Sl
   a.G = C.G;
   a.accumulate = accumulate;
   const int R2 = 1 << C.logR2, R1 = 1 << C.logR1;
-  const size_t smem = cl_smem(variant, f32, P.u16, a.SA, a.SB);
-  if (smem > 227 * 1024) throw unsupported("cluster sketch: residue segments too large for shared memory");
-  (void)R1;
+  int nb = 1;
+  const size_t smem = cl_smem(variant, f32, P.u16, R1, C.log2b, a.SA, a.SB, &nb);
+  if (smem > kClSmemMax) throw unsupported("cluster sketch: residue segments too large for shared memory");
+  if (getenv("CMM_DEBUG"))
+    fprintf(stderr, "[cmm] cluster launch: smem=%zu buffers=%d SA=%lld SB=%lld\n", smem, nb, (long long)a.SA,
+            (long long)a.SB);
   const dim3 grid((unsigned)R2, (unsigned)C.max_clusters, 1);
   ProfScope prof("sketch", s);
   count_launch();
-#define CMM_CL(V, T, CT)                       \
-  do {                                          \
-    cl_kernel_attrs<V, T, CT>(smem);            \
-    cl_launch<V, T, CT>(a, grid, R2, smem, s);  \
+#define CMM_CL(V, T, CT)                                  \
+  do {                                                     \
+    if (nb == 2) {                                         \
+      cl_kernel_attrs<V, T, CT, 2>(smem);                  \
+      cl_launch<V, T, CT, 2>(a, grid, R2, smem, s);        \
+    } else {                                               \
+      cl_kernel_attrs<V, T, CT, 1>(smem);                  \
+      cl_launch<V, T, CT, 1>(a, grid, R2, smem, s);        \
+    }                                                      \
   } while (0)
   if (variant == kVariantFFT) {
     if (f32) { if (P.u16) CMM_CL(0, float, uint16_t); else CMM_CL(0, float, uint32_t); }

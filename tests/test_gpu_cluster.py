@@ -1,0 +1,107 @@
+"""Cluster sketch kernels (FFT and FWHT, FP64 and mixed) against the oracle.
+
+The shapes are chosen so that the automatic dispatch takes the cluster
+kernels (asserted through cmm_last_sketch_kernel) and cover:
+  * clusters of 16 (radix-16 combine split over lane pairs) and of 8;
+  * R1 <= 2 (real DIF weights: the two sides scatter into the real and
+    imaginary parts at once) and R1 > 2 (complex weights, sides one after
+    the other);
+  * two sub-spectrum buffers (FFT) and one (FP64 FWHT);
+  * several work items per cluster and several k-groups;
+  * all-zero rows, which every CTA of a cluster skips, including at the
+    start and end of the inner range (the staged next row must follow);
+  * chunked materialization (accumulating launches).
+Tolerances: FP64 sketch within 1e-11 * max|p| absolute; mixed within
+2e-5 * max|p|.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def capi():
+    from compmatmul_b200 import capi as c
+    return c
+
+
+def kernel():
+    from compmatmul_b200 import lib
+    return lib().cmm_last_sketch_kernel().decode()
+
+
+def check(variant, h, AT, B, d, b, seed, oracle, f32=False):
+    if f32:
+        A32, B32 = AT.astype(np.float32), B.astype(np.float32)
+        p, _ = capi().compressed_product_f32(variant, h, A32, B32, d, b, seed)
+        ref = oracle.compressed_product(variant, h, A32.astype(np.float64), B32.astype(np.float64), d, b, seed)
+        tol = 2e-5
+    else:
+        p, _ = capi().compressed_product(variant, h, AT, B, d, b, seed)
+        ref = oracle.compressed_product(variant, h, AT, B, d, b, seed)
+        tol = 1e-11
+    assert kernel() == "cluster", kernel()
+    np.testing.assert_allclose(p, ref, rtol=0, atol=tol * max(float(np.abs(ref).max()), 1e-300))
+
+
+@pytest.mark.parametrize("b,h", [(1 << 15, None), (1 << 16, "multiply shift"), (1 << 17, "tabulation16"),
+                                 (1 << 18, "tabulation8")])
+def test_fft_fp64(gpu, oracle, b, h):
+    rng = np.random.default_rng(b)
+    AT = rng.standard_normal((23, 300))
+    B = rng.standard_normal((23, 260)) * 1e-2
+    check("fft", h, AT, B, 3, b, 1234, oracle)
+
+
+@pytest.mark.parametrize("b", [1 << 17, 1 << 19])
+def test_fwht_fp64(gpu, oracle, b):
+    rng = np.random.default_rng(b + 1)
+    AT = rng.standard_normal((17, 280))
+    B = rng.standard_normal((17, 310))
+    check("fwht", "multiply add shift", AT, B, 2, b, 77, oracle)
+
+
+def test_fft_many_items_and_groups(gpu, oracle):
+    rng = np.random.default_rng(5)
+    AT = rng.standard_normal((70, 90))
+    B = rng.standard_normal((70, 80))
+    # d = 9 at b = 2^18: more (r1, t) items than co-resident clusters
+    check("fft", None, AT, B, 9, 1 << 18, 9, oracle)
+    # d = 1: the planner splits the inner range into k-groups
+    check("fft", None, AT, B, 1, 1 << 16, 10, oracle)
+
+
+@pytest.mark.parametrize("side", ["A", "B"])
+def test_fft_zero_rows_skipped(gpu, oracle, side):
+    rng = np.random.default_rng(11)
+    AT = rng.standard_normal((41, 200))
+    B = rng.standard_normal((41, 150))
+    M = AT if side == "A" else B
+    M[[0, 1, 2, 7, 8, 20, 39, 40]] = 0.0
+    check("fft", "tabulation8", AT, B, 2, 1 << 16, 3, oracle)
+
+
+def test_fft_all_rows_zero(gpu, oracle):
+    AT = np.zeros((9, 50))
+    B = np.random.default_rng(2).standard_normal((9, 60))
+    p, _ = capi().compressed_product("fft", None, AT, B, 2, 1 << 16, 4)
+    assert kernel() == "cluster"
+    assert float(np.abs(p).max()) == 0.0
+
+
+@pytest.mark.parametrize("variant,b", [("fft", 1 << 16), ("fwht", 1 << 17)])
+def test_chunked_materialization(gpu, oracle, variant, b, monkeypatch):
+    # a small budget runs several materialize + sketch launches that accumulate
+    monkeypatch.setenv("CMM_MATERIALIZE_BYTES", str(300 * 1024))
+    rng = np.random.default_rng(b + 7)
+    AT = rng.standard_normal((64, 400))
+    B = rng.standard_normal((64, 380))
+    check(variant, None, AT, B, 3, b, 21, oracle)
+
+
+@pytest.mark.parametrize("b", [1 << 16, 1 << 18])
+def test_fft_mixed(gpu, oracle, b):
+    rng = np.random.default_rng(b + 3)
+    AT = rng.standard_normal((31, 240))
+    B = rng.standard_normal((31, 220)) * 1e3
+    check("fft", "multiply shift", AT, B, 3, b, 5, oracle, f32=True)
