@@ -68,8 +68,8 @@ def parse():
 # the same kernel on a small case: dram__bytes_read.sum + dram__bytes_write.sum
 # over d * k_chunk * (n_a + n_b) * element bytes, scaled to a full launch by
 # the units it processes (the row reads dominate and grow in proportion).
-# Source: profiles/k_sketch_cluster_fft_small.md (filled in from a capture).
-TRAFFIC_RATIO = {}
+# Source: profiles/k_sketch_cluster_fft_config2_small.md.
+TRAFFIC_RATIO = {("cluster", "fft", "f64"): 1.352 / 1.208}
 
 
 def measured_peaks():
