@@ -157,6 +157,89 @@ static DevBuf upload(const void* h, size_t n, cudaStream_t s) {
   return d;
 }
 
+// second per-thread, per-device stream for host-to-device row copies
+static cudaStream_t copy_stream() {
+  static thread_local std::map<int, cudaStream_t> streams;
+  int dev = 0;
+  CMM_CUDA(cudaGetDevice(&dev));
+  auto it = streams.find(dev);
+  if (it != streams.end()) return it->second;
+  cudaStream_t s;
+  CMM_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  streams[dev] = s;
+  return s;
+}
+
+// Rows of AT and B (the inner index k) copied from host memory while the
+// device works on earlier rows.  The host entry points allocate the device
+// matrices and hand a feed to the sketch; its chunk loop calls wait() before
+// the first use of rows [k0, k0 + c).  The copies run on copy_stream() in
+// pieces of the sketch's chunk size, one event each, issued one piece ahead
+// of the chunk being computed (so pageable host memory, whose copies block
+// the host, still overlaps the previous chunk's kernels).
+class RowFeed {
+ public:
+  RowFeed(const void* hAT, const void* hB, void* dAT, void* dB, int64_t n_a, int64_t n_b,
+          int64_t n_inner, size_t elem, cudaStream_t s)
+      : hAT_(static_cast<const char*>(hAT)), hB_(static_cast<const char*>(hB)),
+        dAT_(static_cast<char*>(dAT)), dB_(static_cast<char*>(dB)), rowA_((size_t)n_a * elem),
+        rowB_((size_t)n_b * elem), n_inner_(n_inner), s_(s), cs_(copy_stream()) {
+    cudaEvent_t ready;  // the device matrices are allocated on s
+    CMM_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+    CMM_CUDA(cudaEventRecord(ready, s));
+    CMM_CUDA(cudaStreamWaitEvent(cs_, ready, 0));
+    CMM_CUDA(cudaEventDestroy(ready));
+  }
+  RowFeed(const RowFeed&) = delete;
+  RowFeed& operator=(const RowFeed&) = delete;
+  // pieces still unwaited (an error ended the sketch early) are ordered
+  // before s's later work, which frees the device matrices
+  ~RowFeed() {
+    for (auto& pc : pieces_) {
+      if (!pc.waited) cudaStreamWaitEvent(s_, pc.ev, 0);
+      cudaEventDestroy(pc.ev);
+    }
+  }
+  // makes s wait until rows [0, k0 + c) are on the device; the first call
+  // fixes the piece length to c
+  void wait(int64_t k0, int64_t c, cudaStream_t s) {
+    if (piece_ == 0) piece_ = c > 0 ? c : 1;
+    const int64_t want = k0 + c + piece_ < n_inner_ ? k0 + c + piece_ : n_inner_;
+    while (issued_ < want) issue();
+    for (auto& pc : pieces_)
+      if (!pc.waited && pc.k0 < k0 + c) {
+        CMM_CUDA(cudaStreamWaitEvent(s, pc.ev, 0));
+        pc.waited = true;
+      }
+  }
+  void wait_all(cudaStream_t s) { wait(0, n_inner_, s); }
+
+ private:
+  struct Piece {
+    int64_t k0;
+    cudaEvent_t ev;
+    bool waited;
+  };
+  void issue() {
+    const int64_t k0 = issued_, c = n_inner_ - k0 < piece_ ? n_inner_ - k0 : piece_;
+    if (rowA_) CMM_CUDA(cudaMemcpyAsync(dAT_ + k0 * rowA_, hAT_ + k0 * rowA_, c * rowA_, cudaMemcpyHostToDevice, cs_));
+    if (rowB_) CMM_CUDA(cudaMemcpyAsync(dB_ + k0 * rowB_, hB_ + k0 * rowB_, c * rowB_, cudaMemcpyHostToDevice, cs_));
+    Piece pc{k0, nullptr, false};
+    CMM_CUDA(cudaEventCreateWithFlags(&pc.ev, cudaEventDisableTiming));
+    CMM_CUDA(cudaEventRecord(pc.ev, cs_));
+    pieces_.push_back(pc);
+    issued_ = k0 + c;
+  }
+  const char* hAT_;
+  const char* hB_;
+  char* dAT_;
+  char* dB_;
+  size_t rowA_, rowB_;
+  int64_t n_inner_, piece_ = 0, issued_ = 0;
+  cudaStream_t s_, cs_;
+  std::vector<Piece> pieces_;
+};
+
 // codes of both sides for keys 0..n_a-1 and 0..n_b-1
 static Codes make_codes(const SketchParams& sp, int64_t n_a, int64_t n_b, cudaStream_t s) {
   DevBuf params = upload(sp.blob.data(), sp.blob.size(), s);
@@ -220,16 +303,21 @@ static bool try_cluster_plan(int variant, bool f32, const Codes& codes, int64_t 
   return cluster_smem_fits(variant, f32, C, plan);
 }
 
+// feed != nullptr: the rows of dAT / dB are still arriving from the host;
+// every chunk waits for its rows (and computes their FFT row scales) first.
 static void sketch_device(int variant, const SketchParams& sp, const Codes& codes, int64_t n_a,
                           int64_t n_inner, int64_t n_b, const double* dAT, const double* dB,
-                          double* dP, cudaStream_t s) {
+                          double* dP, cudaStream_t s, RowFeed* feed = nullptr) {
   const double2* tw = twiddles(sp.b, s);
   const size_t elem = variant == kVariantFFT ? 16 : 8;
   DevBuf scale;
-  if (variant == kVariantFFT) {
-    scale = DevBuf((size_t)(n_inner > 0 ? n_inner : 1) * 4, s);
-    launch_row_scale(dAT, dB, n_a, n_inner, n_b, scale.as<int>(), s);
-  }
+  if (variant == kVariantFFT) scale = DevBuf((size_t)(n_inner > 0 ? n_inner : 1) * 4, s);
+  // rows [k0, k0 + c) usable on s: arrived, and scaled for the FFT
+  auto rows_ready = [&](int64_t k0, int64_t c) {
+    if (feed) feed->wait(k0, c, s);
+    if (variant == kVariantFFT)
+      launch_row_scale(dAT + k0 * n_a, dB + k0 * n_b, n_a, c, n_b, scale.as<int>() + k0, s);
+  };
   ClusterPlan C;
   SlabPlan plan;
   if (n_inner > 0 && try_cluster_plan(variant, false, codes, n_a, n_b, n_inner, sp, C, plan, s)) {
@@ -244,6 +332,7 @@ static void sketch_device(int variant, const SketchParams& sp, const Codes& code
     DevBuf partial((size_t)C.G * sp.d * (size_t)sp.b * elem, s);
     for (int64_t k0 = 0; k0 < n_inner; k0 += kc) {
       const int64_t c = n_inner - k0 < kc ? n_inner - k0 : kc;
+      rows_ready(k0, c);
       launch_materialize(plan, dAT, dB, k0, c, matA.as<double>(), matB.as<double>(), s);
       launch_sketch_cluster(variant, false, C, plan, matA.ptr, matB.ptr, c, scale.as<int>(), k0, tw,
                             partial.ptr, sp.d, k0 > 0 ? 1 : 0, s);
@@ -267,6 +356,7 @@ static void sketch_device(int variant, const SketchParams& sp, const Codes& code
     DevBuf partial((size_t)P.G * sp.d * (size_t)sp.b * elem, s);
     for (int64_t k0 = 0; k0 < n_inner; k0 += kc) {
       const int64_t c = n_inner - k0 < kc ? n_inner - k0 : kc;
+      rows_ready(k0, c);
       launch_materialize(plan, dAT, dB, k0, c, matA.as<double>(), matB.as<double>(), s);
       launch_sketch_v1(P, plan, matA.as<double>(), matB.as<double>(), c, scale.as<int>(), k0, tw,
                        partial.ptr, k0 > 0 ? 1 : 0, s);
@@ -277,6 +367,7 @@ static void sketch_device(int variant, const SketchParams& sp, const Codes& code
   }
   const SketchPlan P = plan_sketch(variant, n_a, n_inner, n_b, sp.d, sp.b, num_sms());
   set_sketch_kernel("small-b");
+  rows_ready(0, n_inner);
   DevBuf partial((size_t)P.G * sp.d * (size_t)sp.b * elem, s);
   launch_sketch_accumulate(P, dAT, dB, codes.a.as<uint32_t>(), codes.b.as<uint32_t>(),
                            scale.as<int>(), tw, partial.ptr, s);
@@ -289,8 +380,10 @@ static void sketch_device(int variant, const SketchParams& sp, const Codes& code
 // FP64 copy of the inputs (on the device).
 static void sketch_device_mixed(int variant, const SketchParams& sp, const Codes& codes,
                                 int64_t n_a, int64_t n_inner, int64_t n_b, const float* dAT,
-                                const float* dB, double* dP, cudaStream_t s) {
+                                const float* dB, double* dP, cudaStream_t s,
+                                RowFeed* feed = nullptr) {
   if (!(n_inner > 0 && sketch_mixed_applicable(variant, sp.b))) {
+    if (feed) feed->wait_all(s);
     DevBuf A64((size_t)n_inner * n_a * 8, s), B64((size_t)n_inner * n_b * 8, s);
     launch_f32_to_f64(dAT, A64.as<double>(), n_inner * n_a, s);
     launch_f32_to_f64(dB, B64.as<double>(), n_inner * n_b, s);
@@ -300,7 +393,11 @@ static void sketch_device_mixed(int variant, const SketchParams& sp, const Codes
   const double2* tw = twiddles(sp.b, s);
   const size_t elem = variant == kVariantFFT ? 16 : 8;
   DevBuf scale((size_t)n_inner * 4, s);
-  if (variant == kVariantFFT) launch_row_scale_f32(dAT, dB, n_a, n_inner, n_b, scale.as<int>(), s);
+  auto rows_ready = [&](int64_t k0, int64_t c) {
+    if (feed) feed->wait(k0, c, s);
+    if (variant == kVariantFFT)
+      launch_row_scale_f32(dAT + k0 * n_a, dB + k0 * n_b, n_a, c, n_b, scale.as<int>() + k0, s);
+  };
   ClusterPlan Cp;
   SlabPlan cplan;
   if (try_cluster_plan(variant, true, codes, n_a, n_b, n_inner, sp, Cp, cplan, s)) {
@@ -315,6 +412,7 @@ static void sketch_device_mixed(int variant, const SketchParams& sp, const Codes
     DevBuf partial((size_t)Cp.G * sp.d * (size_t)sp.b * elem, s);
     for (int64_t k0 = 0; k0 < n_inner; k0 += kc) {
       const int64_t c = n_inner - k0 < kc ? n_inner - k0 : kc;
+      rows_ready(k0, c);
       launch_materialize_f32(plan, dAT, dB, k0, c, matA.as<float>(), matB.as<float>(), s);
       launch_sketch_cluster(variant, true, Cp, plan, matA.ptr, matB.ptr, c, scale.as<int>(), k0, tw,
                             partial.ptr, sp.d, k0 > 0 ? 1 : 0, s);
@@ -336,6 +434,7 @@ static void sketch_device_mixed(int variant, const SketchParams& sp, const Codes
   DevBuf partial((size_t)P.G * sp.d * (size_t)sp.b * elem, s);
   for (int64_t k0 = 0; k0 < n_inner; k0 += kc) {
     const int64_t c = n_inner - k0 < kc ? n_inner - k0 : kc;
+    rows_ready(k0, c);
     launch_materialize_f32(plan, dAT, dB, k0, c, matA.as<float>(), matB.as<float>(), s);
     launch_sketch_mixed(P, plan, matA.as<float>(), matB.as<float>(), c, scale.as<int>(), k0, tw,
                         partial.ptr, k0 > 0 ? 1 : 0, s);
@@ -781,13 +880,13 @@ int cmm_compressed_product_f32(int variant, int hash_kind, int64_t n_a, int64_t 
     const uint64_t sd = pick_seed(has_seed, seed);
     if (seed_out) *seed_out = sd;
     cudaStream_t s = host_stream();
-    DevBuf dAT = upload(AT, (size_t)n_inner * n_a * 4, s);
-    DevBuf dB = upload(B, (size_t)n_inner * n_b * 4, s);
+    DevBuf dAT((size_t)n_inner * n_a * 4, s), dB((size_t)n_inner * n_b * 4, s);
+    RowFeed feed(AT, B, dAT.ptr, dB.ptr, n_a, n_b, n_inner, 4, s);
     SketchParams sp = make_sketch_params(hash_kind, d, b, sd);
     Codes codes = make_codes(sp, n_a, n_b, s);
     DevBuf P((size_t)d * (size_t)b * 8, s);
     sketch_device_mixed(variant, sp, codes, n_a, n_inner, n_b, dAT.as<float>(), dB.as<float>(),
-                        P.as<double>(), s);
+                        P.as<double>(), s, &feed);
     CMM_CUDA(cudaMemcpyAsync(p_out, P.ptr, P.bytes, cudaMemcpyDeviceToHost, s));
     CMM_CUDA(cudaStreamSynchronize(s));
   });
@@ -801,14 +900,14 @@ int cmm_matmul_f32(int variant, int hash_kind, int64_t n_a, int64_t n_inner, int
     check_sizes(n_a, n_inner, n_b);
     const uint64_t sd = pick_seed(has_seed, seed);
     cudaStream_t s = host_stream();
-    DevBuf dAT = upload(AT, (size_t)n_inner * n_a * 4, s);
-    DevBuf dB = upload(B, (size_t)n_inner * n_b * 4, s);
+    DevBuf dAT((size_t)n_inner * n_a * 4, s), dB((size_t)n_inner * n_b * 4, s);
+    RowFeed feed(AT, B, dAT.ptr, dB.ptr, n_a, n_b, n_inner, 4, s);
     DevBuf dC((size_t)n_a * n_b * 8, s);
     SketchParams sp = make_sketch_params(hash_kind, d, b, sd);
     Codes codes = make_codes(sp, n_a, n_b, s);
     DevBuf P((size_t)d * (size_t)b * 8, s);
     sketch_device_mixed(variant, sp, codes, n_a, n_inner, n_b, dAT.as<float>(), dB.as<float>(),
-                        P.as<double>(), s);
+                        P.as<double>(), s, &feed);
     launch_decompress_dense(variant, d, b, n_a, n_b, codes.a.as<uint32_t>(), codes.b.as<uint32_t>(),
                             P.as<double>(), dC.as<double>(), s);
     if (dC.bytes) CMM_CUDA(cudaMemcpyAsync(C, dC.ptr, dC.bytes, cudaMemcpyDeviceToHost, s));
@@ -825,13 +924,13 @@ int cmm_compressed_product(int variant, int hash_kind, int64_t n_a, int64_t n_in
     const uint64_t sd = pick_seed(has_seed, seed);
     if (seed_out) *seed_out = sd;
     cudaStream_t s = host_stream();
-    DevBuf dAT = upload(AT, (size_t)n_inner * n_a * 8, s);
-    DevBuf dB = upload(B, (size_t)n_inner * n_b * 8, s);
+    DevBuf dAT((size_t)n_inner * n_a * 8, s), dB((size_t)n_inner * n_b * 8, s);
+    RowFeed feed(AT, B, dAT.ptr, dB.ptr, n_a, n_b, n_inner, 8, s);
     SketchParams sp = make_sketch_params(hash_kind, d, b, sd);
     Codes codes = make_codes(sp, n_a, n_b, s);
     DevBuf P((size_t)d * (size_t)b * 8, s);
     sketch_device(variant, sp, codes, n_a, n_inner, n_b, dAT.as<double>(), dB.as<double>(),
-                  P.as<double>(), s);
+                  P.as<double>(), s, &feed);
     CMM_CUDA(cudaMemcpyAsync(p_out, P.ptr, P.bytes, cudaMemcpyDeviceToHost, s));
     CMM_CUDA(cudaStreamSynchronize(s));
   });
@@ -844,14 +943,14 @@ int cmm_matmul(int variant, int hash_kind, int64_t n_a, int64_t n_inner, int64_t
     check_sizes(n_a, n_inner, n_b);
     const uint64_t sd = pick_seed(has_seed, seed);
     cudaStream_t s = host_stream();
-    DevBuf dAT = upload(AT, (size_t)n_inner * n_a * 8, s);
-    DevBuf dB = upload(B, (size_t)n_inner * n_b * 8, s);
+    DevBuf dAT((size_t)n_inner * n_a * 8, s), dB((size_t)n_inner * n_b * 8, s);
+    RowFeed feed(AT, B, dAT.ptr, dB.ptr, n_a, n_b, n_inner, 8, s);
     DevBuf dC((size_t)n_a * n_b * 8, s);
     SketchParams sp = make_sketch_params(hash_kind, d, b, sd);
     Codes codes = make_codes(sp, n_a, n_b, s);
     DevBuf P((size_t)d * (size_t)b * 8, s);
     sketch_device(variant, sp, codes, n_a, n_inner, n_b, dAT.as<double>(), dB.as<double>(),
-                  P.as<double>(), s);
+                  P.as<double>(), s, &feed);
     launch_decompress_dense(variant, d, b, n_a, n_b, codes.a.as<uint32_t>(), codes.b.as<uint32_t>(),
                             P.as<double>(), dC.as<double>(), s);
     if (dC.bytes) CMM_CUDA(cudaMemcpyAsync(C, dC.ptr, dC.bytes, cudaMemcpyDeviceToHost, s));
