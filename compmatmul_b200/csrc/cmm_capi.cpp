@@ -303,6 +303,14 @@ static bool try_cluster_plan(int variant, bool f32, const Codes& codes, int64_t 
   return cluster_smem_fits(variant, f32, C, plan);
 }
 
+// Inner indices of the sketch chunk starting at k0.  While rows are still
+// arriving from the host, the first chunk is an eighth of the budget, so the
+// device starts after a short copy.
+static int64_t chunk_len(int64_t k0, int64_t kc, int64_t n_inner, const RowFeed* feed) {
+  const int64_t cmax = (feed && k0 == 0 && kc >= 64) ? kc / 8 : kc;
+  return n_inner - k0 < cmax ? n_inner - k0 : cmax;
+}
+
 // feed != nullptr: the rows of dAT / dB are still arriving from the host;
 // every chunk waits for its rows (and computes their FFT row scales) first.
 static void sketch_device(int variant, const SketchParams& sp, const Codes& codes, int64_t n_a,
@@ -330,8 +338,8 @@ static void sketch_device(int variant, const SketchParams& sp, const Codes& code
     if (kc > n_inner) kc = n_inner;
     DevBuf matA((size_t)sp.d * kc * SA * 8, s), matB((size_t)sp.d * kc * SB * 8, s);
     DevBuf partial((size_t)C.G * sp.d * (size_t)sp.b * elem, s);
-    for (int64_t k0 = 0; k0 < n_inner; k0 += kc) {
-      const int64_t c = n_inner - k0 < kc ? n_inner - k0 : kc;
+    for (int64_t k0 = 0, c = 0; k0 < n_inner; k0 += c) {
+      c = chunk_len(k0, kc, n_inner, feed);
       rows_ready(k0, c);
       launch_materialize(plan, dAT, dB, k0, c, matA.as<double>(), matB.as<double>(), s);
       launch_sketch_cluster(variant, false, C, plan, matA.ptr, matB.ptr, c, scale.as<int>(), k0, tw,
@@ -354,8 +362,8 @@ static void sketch_device(int variant, const SketchParams& sp, const Codes& code
     if (kc > n_inner) kc = n_inner;
     DevBuf matA((size_t)sp.d * kc * SA * 8, s), matB((size_t)sp.d * kc * SB * 8, s);
     DevBuf partial((size_t)P.G * sp.d * (size_t)sp.b * elem, s);
-    for (int64_t k0 = 0; k0 < n_inner; k0 += kc) {
-      const int64_t c = n_inner - k0 < kc ? n_inner - k0 : kc;
+    for (int64_t k0 = 0, c = 0; k0 < n_inner; k0 += c) {
+      c = chunk_len(k0, kc, n_inner, feed);
       rows_ready(k0, c);
       launch_materialize(plan, dAT, dB, k0, c, matA.as<double>(), matB.as<double>(), s);
       launch_sketch_v1(P, plan, matA.as<double>(), matB.as<double>(), c, scale.as<int>(), k0, tw,
@@ -410,8 +418,8 @@ static void sketch_device_mixed(int variant, const SketchParams& sp, const Codes
     if (kc > n_inner) kc = n_inner;
     DevBuf matA((size_t)sp.d * kc * SA * 4, s), matB((size_t)sp.d * kc * SB * 4, s);
     DevBuf partial((size_t)Cp.G * sp.d * (size_t)sp.b * elem, s);
-    for (int64_t k0 = 0; k0 < n_inner; k0 += kc) {
-      const int64_t c = n_inner - k0 < kc ? n_inner - k0 : kc;
+    for (int64_t k0 = 0, c = 0; k0 < n_inner; k0 += c) {
+      c = chunk_len(k0, kc, n_inner, feed);
       rows_ready(k0, c);
       launch_materialize_f32(plan, dAT, dB, k0, c, matA.as<float>(), matB.as<float>(), s);
       launch_sketch_cluster(variant, true, Cp, plan, matA.ptr, matB.ptr, c, scale.as<int>(), k0, tw,
@@ -432,8 +440,8 @@ static void sketch_device_mixed(int variant, const SketchParams& sp, const Codes
   if (kc > n_inner) kc = n_inner;
   DevBuf matA((size_t)sp.d * kc * SA * 4, s), matB((size_t)sp.d * kc * SB * 4, s);
   DevBuf partial((size_t)P.G * sp.d * (size_t)sp.b * elem, s);
-  for (int64_t k0 = 0; k0 < n_inner; k0 += kc) {
-    const int64_t c = n_inner - k0 < kc ? n_inner - k0 : kc;
+  for (int64_t k0 = 0, c = 0; k0 < n_inner; k0 += c) {
+    c = chunk_len(k0, kc, n_inner, feed);
     rows_ready(k0, c);
     launch_materialize_f32(plan, dAT, dB, k0, c, matA.as<float>(), matB.as<float>(), s);
     launch_sketch_mixed(P, plan, matA.as<float>(), matB.as<float>(), c, scale.as<int>(), k0, tw,
@@ -444,6 +452,49 @@ static void sketch_device_mixed(int variant, const SketchParams& sp, const Codes
 }
 
 static uint64_t pick_seed(int has_seed, uint64_t seed) { return has_seed ? seed : time_seed(); }
+
+// The dense estimate comes back to the host in row blocks: every block's
+// decompression is enqueued on s first, then each block's copy on
+// copy_stream() after its event, so the copies overlap the decompression of
+// the later blocks (with pageable host memory too, whose copies block the
+// host).  Returns when C is on the host.
+static void decompress_to_host(int variant, int d, int b, int64_t n_a, int64_t n_b, const Codes& codes,
+                               const double* dP, double* dC, double* C, cudaStream_t s) {
+  struct Join {  // s waits for the copies before anything later (frees) runs on it
+    cudaStream_t s, cs;
+    std::vector<cudaEvent_t> ev;
+    ~Join() {
+      cudaEvent_t done;
+      if (cudaEventCreateWithFlags(&done, cudaEventDisableTiming) == cudaSuccess) {
+        cudaEventRecord(done, cs);
+        cudaStreamWaitEvent(s, done, 0);
+        cudaEventDestroy(done);
+      }
+      for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    }
+  } join{s, copy_stream(), {}};
+  if (n_a > 0 && n_b > 0) {
+    int64_t rows = (n_a + 7) / 8;
+    rows = (rows + 15) / 16 * 16;
+    for (int64_t i0 = 0; i0 < n_a; i0 += rows) {
+      const int64_t r = n_a - i0 < rows ? n_a - i0 : rows;
+      launch_decompress_dense_rows(variant, d, b, n_a, n_b, i0, r, codes.a.as<uint32_t>(), codes.b.as<uint32_t>(),
+                                   dP, dC + i0 * n_b, s);
+      cudaEvent_t e;
+      CMM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      join.ev.push_back(e);
+      CMM_CUDA(cudaEventRecord(e, s));
+    }
+    size_t blk = 0;
+    for (int64_t i0 = 0; i0 < n_a; i0 += rows, ++blk) {
+      const int64_t r = n_a - i0 < rows ? n_a - i0 : rows;
+      CMM_CUDA(cudaStreamWaitEvent(join.cs, join.ev[blk], 0));
+      CMM_CUDA(cudaMemcpyAsync(C + i0 * n_b, dC + i0 * n_b, (size_t)r * n_b * 8, cudaMemcpyDeviceToHost, join.cs));
+    }
+  }
+  CMM_CUDA(cudaStreamSynchronize(join.cs));
+  CMM_CUDA(cudaStreamSynchronize(s));
+}
 
 // ------------------------------------------------------- instrumentation
 static std::atomic<int64_t> g_launches{0};
@@ -908,10 +959,7 @@ int cmm_matmul_f32(int variant, int hash_kind, int64_t n_a, int64_t n_inner, int
     DevBuf P((size_t)d * (size_t)b * 8, s);
     sketch_device_mixed(variant, sp, codes, n_a, n_inner, n_b, dAT.as<float>(), dB.as<float>(),
                         P.as<double>(), s, &feed);
-    launch_decompress_dense(variant, d, b, n_a, n_b, codes.a.as<uint32_t>(), codes.b.as<uint32_t>(),
-                            P.as<double>(), dC.as<double>(), s);
-    if (dC.bytes) CMM_CUDA(cudaMemcpyAsync(C, dC.ptr, dC.bytes, cudaMemcpyDeviceToHost, s));
-    CMM_CUDA(cudaStreamSynchronize(s));
+    decompress_to_host(variant, d, b, n_a, n_b, codes, P.as<double>(), dC.as<double>(), C, s);
   });
 }
 
@@ -951,10 +999,7 @@ int cmm_matmul(int variant, int hash_kind, int64_t n_a, int64_t n_inner, int64_t
     DevBuf P((size_t)d * (size_t)b * 8, s);
     sketch_device(variant, sp, codes, n_a, n_inner, n_b, dAT.as<double>(), dB.as<double>(),
                   P.as<double>(), s, &feed);
-    launch_decompress_dense(variant, d, b, n_a, n_b, codes.a.as<uint32_t>(), codes.b.as<uint32_t>(),
-                            P.as<double>(), dC.as<double>(), s);
-    if (dC.bytes) CMM_CUDA(cudaMemcpyAsync(C, dC.ptr, dC.bytes, cudaMemcpyDeviceToHost, s));
-    CMM_CUDA(cudaStreamSynchronize(s));
+    decompress_to_host(variant, d, b, n_a, n_b, codes, P.as<double>(), dC.as<double>(), C, s);
   });
 }
 

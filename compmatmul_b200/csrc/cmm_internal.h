@@ -141,6 +141,9 @@ void launch_finalize(const SketchPlan& P, const void* dPartial, const double2* d
 void launch_decompress_dense(int variant, int d, int b, int64_t n_a, int64_t n_b,
                              const uint32_t* dCodesA, const uint32_t* dCodesB, const double* dP,
                              double* dC, cudaStream_t s);
+void launch_decompress_dense_rows(int variant, int d, int b, int64_t n_a, int64_t n_b, int64_t i0,
+                                  int64_t rows, const uint32_t* dCodesA, const uint32_t* dCodesB,
+                                  const double* dP, double* dCrows, cudaStream_t s);
 
 // codes are d x count, one column per listed (i, j) entry
 void launch_decompress_list(int variant, int d, int b, int64_t count, const uint32_t* dCodesI,

@@ -46,14 +46,14 @@ template <int VARIANT, int D>
 __global__ void __launch_bounds__(kDecThreads) k_decompress(const uint32_t* __restrict__ cA,
                                                             const uint32_t* __restrict__ cB,
                                                             const double* __restrict__ p, int b,
-                                                            int64_t n_a, int64_t n_b,
+                                                            int64_t n_a, int64_t n_b, int64_t lda,
                                                             double* __restrict__ C) {
   __shared__ uint32_t sA[D][kDecRows];
   const int64_t j = (int64_t)blockIdx.x * kDecThreads + threadIdx.x;
   const int64_t i0 = (int64_t)blockIdx.y * kDecRows;
   for (int e = threadIdx.x; e < D * kDecRows; e += kDecThreads) {
     const int t = e / kDecRows, ii = e % kDecRows;
-    sA[t][ii] = (i0 + ii < n_a) ? cA[(size_t)t * n_a + i0 + ii] : 0u;
+    sA[t][ii] = (i0 + ii < n_a) ? cA[(size_t)t * lda + i0 + ii] : 0u;
   }
   __syncthreads();
   if (j >= n_b) return;
@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(kDecThreads) k_decompress(const uint32_t* __re
 template <int VARIANT>
 __global__ void k_decompress_generic(const uint32_t* __restrict__ cA, const uint32_t* __restrict__ cB,
                                      const double* __restrict__ p, int d, int b, int64_t n_a,
-                                     int64_t n_b, double* __restrict__ C) {
+                                     int64_t n_b, int64_t lda, double* __restrict__ C) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t i = blockIdx.y;
   if (j >= n_b || i >= n_a) return;
@@ -82,10 +82,10 @@ __global__ void k_decompress_generic(const uint32_t* __restrict__ cA, const uint
   const int mid = d / 2;
   double ans = 0.0;
   for (int a = 0; a < d; ++a) {
-    const double va = estimate<VARIANT>(p + (size_t)a * b, cA[(size_t)a * n_a + i], cB[(size_t)a * n_b + j], mask);
+    const double va = estimate<VARIANT>(p + (size_t)a * b, cA[(size_t)a * lda + i], cB[(size_t)a * n_b + j], mask);
     int lt = 0, le = 0;
     for (int t = 0; t < d; ++t) {
-      const double vt = estimate<VARIANT>(p + (size_t)t * b, cA[(size_t)t * n_a + i], cB[(size_t)t * n_b + j], mask);
+      const double vt = estimate<VARIANT>(p + (size_t)t * b, cA[(size_t)t * lda + i], cB[(size_t)t * n_b + j], mask);
       lt += vt < va;
       le += vt <= va;
     }
@@ -96,16 +96,16 @@ __global__ void k_decompress_generic(const uint32_t* __restrict__ cA, const uint
 
 template <int VARIANT, int D>
 static void dec_launch(const uint32_t* cA, const uint32_t* cB, const double* p, int b, int64_t n_a,
-                       int64_t n_b, double* C, cudaStream_t s) {
+                       int64_t n_b, int64_t lda, double* C, cudaStream_t s) {
   dim3 grid((unsigned)((n_b + kDecThreads - 1) / kDecThreads), (unsigned)((n_a + kDecRows - 1) / kDecRows));
-  k_decompress<VARIANT, D><<<grid, kDecThreads, 0, s>>>(cA, cB, p, b, n_a, n_b, C);
+  k_decompress<VARIANT, D><<<grid, kDecThreads, 0, s>>>(cA, cB, p, b, n_a, n_b, lda, C);
 }
 
 template <int VARIANT>
 static void dec_dispatch(int d, const uint32_t* cA, const uint32_t* cB, const double* p, int b,
-                         int64_t n_a, int64_t n_b, double* C, cudaStream_t s) {
+                         int64_t n_a, int64_t n_b, int64_t lda, double* C, cudaStream_t s) {
   switch (d) {
-#define CMM_DEC_CASE(D) case D: dec_launch<VARIANT, D>(cA, cB, p, b, n_a, n_b, C, s); return;
+#define CMM_DEC_CASE(D) case D: dec_launch<VARIANT, D>(cA, cB, p, b, n_a, n_b, lda, C, s); return;
     CMM_DEC_CASE(1) CMM_DEC_CASE(2) CMM_DEC_CASE(3) CMM_DEC_CASE(4) CMM_DEC_CASE(5)
     CMM_DEC_CASE(6) CMM_DEC_CASE(7) CMM_DEC_CASE(8) CMM_DEC_CASE(9) CMM_DEC_CASE(10)
     CMM_DEC_CASE(11) CMM_DEC_CASE(12) CMM_DEC_CASE(13) CMM_DEC_CASE(14) CMM_DEC_CASE(15)
@@ -114,7 +114,7 @@ static void dec_dispatch(int d, const uint32_t* cA, const uint32_t* cB, const do
     default: {
       if (n_a > 2147483647LL) throw unsupported("n_a too large for the generic-d decompression");
       dim3 grid((unsigned)((n_b + 255) / 256), (unsigned)n_a);
-      k_decompress_generic<VARIANT><<<grid, 256, 0, s>>>(cA, cB, p, d, b, n_a, n_b, C);
+      k_decompress_generic<VARIANT><<<grid, 256, 0, s>>>(cA, cB, p, d, b, n_a, n_b, lda, C);
     }
   }
 }
@@ -126,8 +126,22 @@ void launch_decompress_dense(int variant, int d, int b, int64_t n_a, int64_t n_b
   if ((n_a + kDecRows - 1) / kDecRows > 2147483647LL) throw unsupported("n_a too large");
   ProfScope prof("decompress", s);
   count_launch();
-  if (variant == kVariantFFT) dec_dispatch<kVariantFFT>(d, dCodesA, dCodesB, dP, b, n_a, n_b, dC, s);
-  else dec_dispatch<kVariantFWHT>(d, dCodesA, dCodesB, dP, b, n_a, n_b, dC, s);
+  if (variant == kVariantFFT) dec_dispatch<kVariantFFT>(d, dCodesA, dCodesB, dP, b, n_a, n_b, n_a, dC, s);
+  else dec_dispatch<kVariantFWHT>(d, dCodesA, dCodesB, dP, b, n_a, n_b, n_a, dC, s);
+  CMM_CUDA(cudaGetLastError());
+}
+
+// rows [i0, i0 + rows) of the dense estimate into dCrows (rows x n_b)
+void launch_decompress_dense_rows(int variant, int d, int b, int64_t n_a, int64_t n_b, int64_t i0,
+                                  int64_t rows, const uint32_t* dCodesA, const uint32_t* dCodesB,
+                                  const double* dP, double* dCrows, cudaStream_t s) {
+  if (rows <= 0 || n_b <= 0) return;
+  if (i0 < 0 || i0 + rows > n_a) throw invalid_argument("decompression rows out of range");
+  if ((rows + kDecRows - 1) / kDecRows > 2147483647LL) throw unsupported("n_a too large");
+  ProfScope prof("decompress", s);
+  count_launch();
+  if (variant == kVariantFFT) dec_dispatch<kVariantFFT>(d, dCodesA + i0, dCodesB, dP, b, rows, n_b, n_a, dCrows, s);
+  else dec_dispatch<kVariantFWHT>(d, dCodesA + i0, dCodesB, dP, b, rows, n_b, n_a, dCrows, s);
   CMM_CUDA(cudaGetLastError());
 }
 
