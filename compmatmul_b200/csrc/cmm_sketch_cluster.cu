@@ -14,12 +14,17 @@
 //    cluster, reading the other CTAs' shared memory (DSMEM): CTA r2 owns the
 //    frequencies of L / R2 sub-spectrum positions and accumulates
 //    Z^2 (FFT, z = alpha x + i beta y) or X * Y (FWHT) for them over k.
-//  Two cluster barriers per inner index keep the sub-spectra alive while
-//  they are read.  Every CTA of a cluster runs the same k loop, so all of
-//  them reach every barrier.
+//  With two sub-spectrum buffers (when they fit in shared memory) one
+//  cluster barrier per inner index both publishes the new sub-spectra and
+//  retires the reads of the buffer written next; with one buffer a second
+//  barrier follows the combine.  Every CTA of a cluster runs the same k
+//  sequence (all-zero rows are skipped by all of them), so all of them
+//  reach every barrier.
+//  The next row's segments are staged with cp.async while the current one
+//  is transformed and combined.
 // Instantiations: FFT/FWHT x FP64/FP32 (FP32 = mixed precision: FP32 data,
 // two-sum compensated accumulation, tensor-core Hadamard-16 stages for the
-// FWHT, FP64 partials).
+// FWHT, FP64 partials) x one or two buffers.
 #include <cooperative_groups.h>
 #include <cuda_bf16.h>
 
