@@ -39,7 +39,7 @@ EXPORTED = [
     "cmm_last_sketch_kernel", "cmm_probe_fma_tflops", "cmm_batch_create", "cmm_batch_run",
     "cmm_batch_info", "cmm_batch_config", "cmm_batch_destroy", "cmm_server_create", "cmm_server_submit",
     "cmm_server_wait", "cmm_server_stats_get", "cmm_server_destroy", "cmm_dev_decompress_entries",
-    "cmm_dev_sketch_topk",
+    "cmm_dev_sketch_topk", "cmm_rng_seed", "cmm_rng_next", "cmm_time_millis", "cmm_hash_params",
 ]
 
 
@@ -104,9 +104,16 @@ def lib():
     L.cmm_profile_reset.restype = None
     L.cmm_profile_read.argtypes = [_C.c_char_p, _C.POINTER(_C.c_double), _C.POINTER(i64)]
     L.cmm_launch_count.restype = i64
+    L.cmm_rng_seed.argtypes = [u64, vp]
+    L.cmm_rng_seed.restype = None
+    L.cmm_rng_next.argtypes = [vp]
+    L.cmm_rng_next.restype = u64
+    L.cmm_time_millis.restype = u64
+    L.cmm_hash_params.argtypes = [i32, i32, u64, u64, vp, _C.c_size_t]
     for name in EXPORTED:
         if name not in ("cmm_last_error", "cmm_version", "cmm_profile_enable", "cmm_last_sketch_kernel",
-                        "cmm_profile_reset", "cmm_launch_count"):
+                        "cmm_profile_reset", "cmm_launch_count", "cmm_rng_seed", "cmm_rng_next",
+                        "cmm_time_millis"):
             getattr(L, name).restype = i32
     _lib = L
     return L

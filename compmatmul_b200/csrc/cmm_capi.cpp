@@ -1062,4 +1062,39 @@ int cmm_hash_codes(int hash_kind, int d, int b, uint64_t seed, int side, int64_t
   });
 }
 
+// --------------------------------------------- host-side rng and hash draws
+// No CUDA call: these give C++ callers of the header entry points the
+// reference's rng and hash objects (rng.hpp, hashing.hpp) bit for bit.
+
+void cmm_rng_seed(uint64_t seed, uint64_t* state) {
+  const Xoshiro256ss r(seed);
+  for (int i = 0; i < 4; ++i) state[i] = r.s[i];
+}
+
+uint64_t cmm_rng_next(uint64_t* state) {
+  Xoshiro256ss r(0);
+  for (int i = 0; i < 4; ++i) r.s[i] = state[i];
+  const uint64_t v = r();
+  for (int i = 0; i < 4; ++i) state[i] = r.s[i];
+  return v;
+}
+
+uint64_t cmm_time_millis(void) { return time_millis(); }
+
+int cmm_hash_params(int hash_kind, int n, uint64_t buckets, uint64_t seed, void* out, size_t out_bytes) {
+  return guarded([&] {
+    if (hash_kind < 0 || hash_kind > 3) throw cmm::invalid_argument("unknown hash kind");
+    if (buckets == 0 || (buckets & (buckets - 1)) != 0)
+      throw cmm::invalid_argument("The number of buckets must be a power of 2");
+    if (n < 0) throw cmm::invalid_argument("negative function count");
+    const size_t need = hash_param_bytes(hash_kind) * (size_t)n;
+    if (out_bytes < need)
+      throw cmm::invalid_argument("output buffer holds " + std::to_string(out_bytes) + " bytes, " +
+                                  std::to_string(need) + " needed");
+    if (n == 0) return;
+    const std::vector<uint8_t> v = draw_hash_params(hash_kind, n, seed);
+    std::memcpy(out, v.data(), need);
+  });
+}
+
 }  // extern "C"

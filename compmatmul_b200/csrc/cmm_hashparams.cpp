@@ -36,11 +36,13 @@ uint64_t Xoshiro256ss::operator()() {
   return result;
 }
 
-uint64_t time_seed() {
+uint64_t time_millis() {
   using namespace std::chrono;
-  const uint64_t ms =
-      (uint64_t)duration_cast<milliseconds>(system_clock::now().time_since_epoch()).count();
-  Xoshiro256ss r(ms);
+  return (uint64_t)duration_cast<milliseconds>(system_clock::now().time_since_epoch()).count();
+}
+
+uint64_t time_seed() {
+  Xoshiro256ss r(time_millis());
   return r();
 }
 

@@ -41,6 +41,8 @@ struct Xoshiro256ss {
   uint64_t operator()();
 };
 
+// Milliseconds since the epoch (rng.hpp:40-44).
+uint64_t time_millis();
 // Seed used when the caller gives none: rng()() with the ms clock seed
 // (rng.hpp:40-44, 54-56; matmul_fft.hpp:30-32).
 uint64_t time_seed();

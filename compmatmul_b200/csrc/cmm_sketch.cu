@@ -5,7 +5,7 @@
 // of B into b buckets, transform both, multiply pointwise, accumulate over
 // k, and finally inverse-transform the d accumulated spectra into p (d x b).
 //
-// B200 formulation (see DESIGN.md for the derivation):
+// B200 formulation:
 //  * Hash codes are precomputed once per call, one u32 per (t, index):
 //    bucket | (sign == +1) << 31 (k_hash_codes).  The reference re-hashes
 //    per (k, t, i); the values are identical.

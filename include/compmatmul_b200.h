@@ -104,6 +104,30 @@ int cmm_hash_codes(int hash_kind, int d, int b, uint64_t seed, int side, int64_t
                    uint32_t* codes_out);
 
 /* ---------------------------------------------------------------------
+ * Host-side random stream and hash draws (no CUDA call).  They let the C++
+ * header entry points hand out the reference's rng and hash objects
+ * (matmul_sketch::h1/h2/s1/s2) with the same parameters bit for bit.
+ * ------------------------------------------------------------------- */
+
+/* Replaces compmatmul::splitmix64 + rng::rng(seed) (rng.hpp:26-33, 54-57):
+ * the four xoshiro256** state words seeded from `seed`. */
+void cmm_rng_seed(uint64_t seed, uint64_t* state4);
+/* Replaces rng::operator() (rng.hpp:59-72): the next 64-bit value; steps
+ * the state in place. */
+uint64_t cmm_rng_next(uint64_t* state4);
+/* Replaces compmatmul::current_system_time_millis (rng.hpp:40-44), the
+ * seed of rng() without one. */
+uint64_t cmm_time_millis(void);
+/* Replaces Hash::draw(n, buckets, seed) of hashing.hpp (multiply_shift
+ * :69-87, multiply_add_shift :145-160, tabulation :277-295): parameters of
+ * n functions from one stream seeded with `seed`, packed back to back:
+ * multiply shift -> u64 a; multiply add shift -> u64 a, u64 b;
+ * tabulation8 -> u32 T[4][256]; tabulation16 -> u32 T[2][65536].
+ * buckets must be a power of two (the reference's message otherwise). */
+int cmm_hash_params(int hash_kind, int n, uint64_t buckets, uint64_t seed, void* out,
+                    size_t out_bytes);
+
+/* ---------------------------------------------------------------------
  * Device-pointer, stream-ordered entry points (no reference twin: the
  * reference is host-only).  All pointers are device pointers.
  * ------------------------------------------------------------------- */

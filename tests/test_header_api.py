@@ -1,6 +1,7 @@
 """The C++ header entry points (include/compmatmul_b200.hpp): the program
-builds here (no GPU needed) and runs the reference's small exact products
-on the GPU."""
+builds here, checks the host-side hash objects here (no GPU needed) and
+runs the reference's small exact products through the sketch type on the
+GPU."""
 import os
 import subprocess
 
@@ -20,6 +21,15 @@ def build(tmp_path):
 
 def test_header_compiles(tmp_path):
     assert os.path.exists(build(tmp_path))
+
+
+def test_header_hash_objects_match_reference(tmp_path):
+    """Host-side part (no GPU): rng, the hash families, sign hashes and the
+    sketch's drawn functions against the reference's own values."""
+    exe = build(tmp_path)
+    r = subprocess.run([exe, "hash"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.strip().endswith("ok")
 
 
 @pytest.mark.gpu
