@@ -63,7 +63,25 @@ int num_sms() {
   return n;
 }
 
-// w[j] = exp(-2 pi i j / b), built in long double, cached per (device, b)
+// w[j] = exp(-2 pi i j / b), j < b, built in long double once per b on the
+// host (kept for the process: the device tables and the allocation-free
+// entry point copy from it)
+static const std::vector<double2>& host_twiddles(int b) {
+  static std::mutex mu;
+  static std::map<int, std::vector<double2>> cache;
+  std::lock_guard<std::mutex> g(mu);
+  auto it = cache.find(b);
+  if (it != cache.end()) return it->second;
+  std::vector<double2> h((size_t)b);
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  for (int j = 0; j < b; ++j) {
+    const long double a = -two_pi * (long double)j / (long double)b;
+    h[(size_t)j] = make_double2((double)cosl(a), (double)sinl(a));
+  }
+  return cache.emplace(b, std::move(h)).first->second;
+}
+
+// the same table on the device, cached per (device, b)
 const double2* twiddles(int b, cudaStream_t s) {
   static std::mutex mu;
   static std::map<std::pair<int, int>, double2*> cache;
@@ -73,12 +91,7 @@ const double2* twiddles(int b, cudaStream_t s) {
   auto key = std::make_pair(dev, b);
   auto it = cache.find(key);
   if (it != cache.end()) return it->second;
-  std::vector<double2> h((size_t)b);
-  const long double two_pi = 6.283185307179586476925286766559005768L;
-  for (int j = 0; j < b; ++j) {
-    const long double a = -two_pi * (long double)j / (long double)b;
-    h[(size_t)j] = make_double2((double)cosl(a), (double)sinl(a));
-  }
+  const std::vector<double2>& h = host_twiddles(b);
   double2* d = nullptr;
   CMM_CUDA(cudaMalloc(&d, sizeof(double2) * (size_t)b));
   CMM_CUDA(cudaMemcpyAsync(d, h.data(), sizeof(double2) * (size_t)b, cudaMemcpyHostToDevice, s));
@@ -297,9 +310,18 @@ static bool try_cluster_plan(int variant, bool f32, const Codes& codes, int64_t 
   } catch (const unsupported&) {
     return false;
   }
-  plan = make_residue_plan(codes.a.as<uint32_t>(), codes.b.as<uint32_t>(), n_a, n_b, sp.d, sp.b,
-                           C.logL, C.logR2, s);
+  plan = make_owner_plan(codes.a.as<uint32_t>(), codes.b.as<uint32_t>(), n_a, n_b, sp.d, sp.b, C.logL,
+                         C.logR2, variant, s);
   return cluster_smem_fits(variant, f32, C, plan);
+}
+
+// Inner indices per cluster-kernel launch: all of them for device inputs;
+// with rows still arriving from the host, an eighth (at least 64), so the
+// kernels of one piece overlap the copies of the next.
+static int64_t cluster_chunk(int64_t n_inner, const RowFeed* feed) {
+  if (!feed) return n_inner;
+  const int64_t c = n_inner / 8;
+  return c < 64 ? (n_inner < 64 ? n_inner : 64) : c;
 }
 
 // Inner indices of the sketch chunk starting at k0.  While rows are still
@@ -328,21 +350,15 @@ static void sketch_device(int variant, const SketchParams& sp, const Codes& code
   ClusterPlan C;
   SlabPlan plan;
   if (n_inner > 0 && try_cluster_plan(variant, false, codes, n_a, n_b, n_inner, sp, C, plan, s)) {
-    // residue plan + per-chunk materialized rows + cluster kernels
+    // owner plan + cluster kernels reading the rows in place
     set_sketch_kernel("cluster");
-    const int64_t SA = plan.slots_a(), SB = plan.slots_b();
-    const size_t per_row = (size_t)sp.d * (size_t)(SA + SB) * 8;
-    int64_t kc = (int64_t)(materialize_budget() / per_row);
-    if (kc < 1) kc = 1;
-    if (kc > n_inner) kc = n_inner;
-    DevBuf matA((size_t)sp.d * kc * SA * 8, s), matB((size_t)sp.d * kc * SB * 8, s);
+    const int64_t kc = cluster_chunk(n_inner, feed);
     DevBuf partial((size_t)C.G * sp.d * (size_t)sp.b * elem, s);
     for (int64_t k0 = 0, c = 0; k0 < n_inner; k0 += c) {
       c = chunk_len(k0, kc, n_inner, feed);
       rows_ready(k0, c);
-      launch_materialize(plan, dAT, dB, k0, c, matA.as<double>(), matB.as<double>(), s);
-      launch_sketch_cluster(variant, false, C, plan, matA.ptr, matB.ptr, c, scale.as<int>(), k0, tw,
-                            partial.ptr, sp.d, k0 > 0 ? 1 : 0, s);
+      launch_sketch_cluster(variant, false, C, plan, dAT, dB, c, scale.as<int>(), k0, tw, partial.ptr, sp.d,
+                            k0 > 0 ? 1 : 0, s);
     }
     DevBuf work(2 * (size_t)sp.d * (size_t)sp.b * 16, s);
     launch_finalize_natural(variant, sp.d, sp.b, C.G, partial.ptr, tw, work.ptr, dP, s);
@@ -409,20 +425,13 @@ static void sketch_device_mixed(int variant, const SketchParams& sp, const Codes
   SlabPlan cplan;
   if (try_cluster_plan(variant, true, codes, n_a, n_b, n_inner, sp, Cp, cplan, s)) {
     set_sketch_kernel("cluster");
-    SlabPlan& plan = cplan;
-    const int64_t SA = plan.slots_a(), SB = plan.slots_b();
-    const size_t per_row = (size_t)sp.d * (size_t)(SA + SB) * 4;
-    int64_t kc = (int64_t)(materialize_budget() / per_row);
-    if (kc < 1) kc = 1;
-    if (kc > n_inner) kc = n_inner;
-    DevBuf matA((size_t)sp.d * kc * SA * 4, s), matB((size_t)sp.d * kc * SB * 4, s);
+    const int64_t kc = cluster_chunk(n_inner, feed);
     DevBuf partial((size_t)Cp.G * sp.d * (size_t)sp.b * elem, s);
     for (int64_t k0 = 0, c = 0; k0 < n_inner; k0 += c) {
       c = chunk_len(k0, kc, n_inner, feed);
       rows_ready(k0, c);
-      launch_materialize_f32(plan, dAT, dB, k0, c, matA.as<float>(), matB.as<float>(), s);
-      launch_sketch_cluster(variant, true, Cp, plan, matA.ptr, matB.ptr, c, scale.as<int>(), k0, tw,
-                            partial.ptr, sp.d, k0 > 0 ? 1 : 0, s);
+      launch_sketch_cluster(variant, true, Cp, cplan, dAT, dB, c, scale.as<int>(), k0, tw, partial.ptr, sp.d,
+                            k0 > 0 ? 1 : 0, s);
     }
     DevBuf work(2 * (size_t)sp.d * (size_t)sp.b * 16, s);
     launch_finalize_natural(variant, sp.d, sp.b, Cp.G, partial.ptr, tw, work.ptr, dP, s);
@@ -741,17 +750,9 @@ int cmm_dev_compressed_product_noalloc(int variant, int hash_kind, int64_t n_a, 
     uint32_t* cb = reinterpret_cast<uint32_t*>(base + o_cb);
     launch_hash_codes(hash_kind, base + o_blob, base + o_blob + 2 * set, d, sp.log2b, n_a, ca, s);
     launch_hash_codes(hash_kind, base + o_blob + set, base + o_blob + 3 * set, d, sp.log2b, n_b, cb, s);
-    {
-      // w[j] = exp(-2 pi i j / b) in long double, as the cached table
-      std::vector<double2> h((size_t)b);
-      const long double two_pi = 6.283185307179586476925286766559005768L;
-      for (int j = 0; j < b; ++j) {
-        const long double a = -two_pi * (long double)j / (long double)b;
-        h[(size_t)j] = make_double2((double)cosl(a), (double)sinl(a));
-      }
-      CMM_CUDA(cudaMemcpyAsync(base + o_tw, h.data(), sizeof(double2) * (size_t)b,
-                               cudaMemcpyHostToDevice, s));
-    }
+    // w[j] = exp(-2 pi i j / b): the process-wide host table (built once per b)
+    CMM_CUDA(cudaMemcpyAsync(base + o_tw, host_twiddles(b).data(), sizeof(double2) * (size_t)b,
+                             cudaMemcpyHostToDevice, s));
     const double2* tw = reinterpret_cast<const double2*>(base + o_tw);
     int* scale = fft ? reinterpret_cast<int*>(base + o_scale) : nullptr;
     if (fft) launch_row_scale(dAT, dB, n_a, n_inner, n_b, scale, s);

@@ -10,7 +10,8 @@ kernels (asserted through cmm_last_sketch_kernel) and cover:
   * several work items per cluster and several k-groups;
   * all-zero rows, which every CTA of a cluster skips, including at the
     start and end of the inner range (the staged next row must follow);
-  * chunked materialization (accumulating launches).
+  * chunked launches over streamed host rows (accumulating partials);
+  * rows gathered in place from AT and B (no per-repetition copies).
 Tolerances: FP64 sketch within 1e-11 * max|p| absolute; mixed within
 2e-5 * max|p|.
 """
@@ -89,14 +90,29 @@ def test_fft_all_rows_zero(gpu, oracle):
     assert float(np.abs(p).max()) == 0.0
 
 
-@pytest.mark.parametrize("variant,b", [("fft", 1 << 16), ("fwht", 1 << 17)])
-def test_chunked_materialization(gpu, oracle, variant, b, monkeypatch):
-    # a small budget runs several materialize + sketch launches that accumulate
-    monkeypatch.setenv("CMM_MATERIALIZE_BYTES", str(300 * 1024))
+@pytest.mark.parametrize("variant,b", [("fft", 1 << 15), ("fwht", 1 << 16)])
+def test_chunked_launches_accumulate(gpu, oracle, variant, b):
+    # the host entry point streams the rows in chunks (an eighth of the inner
+    # range, the first one an eighth of that): several cluster launches,
+    # each adding to the k-group partials of the previous ones
     rng = np.random.default_rng(b + 7)
-    AT = rng.standard_normal((64, 400))
-    B = rng.standard_normal((64, 380))
+    AT = rng.standard_normal((600, 120))
+    B = rng.standard_normal((600, 100))
+    AT[[0, 8, 9, 599]] = 0.0  # skipped rows at chunk edges
     check(variant, None, AT, B, 3, b, 21, oracle)
+
+
+def test_gather_reads_rows_in_place(gpu, oracle):
+    """The kernels gather each row's segment from AT and B directly, with
+    the sign applied per slot: rows of very different scales in A and B
+    (the FFT row balance) and a planted large entry, both variants."""
+    rng = np.random.default_rng(19)
+    AT = rng.standard_normal((50, 333)) * np.logspace(-3, 3, 50)[:, None]
+    B = rng.standard_normal((50, 277)) * np.logspace(3, -3, 50)[:, None]
+    AT[10, 5] += 1e4
+    B[10, 7] += 1e4
+    check("fft", None, AT, B, 5, 1 << 16, 8, oracle)
+    check("fwht", None, AT, B, 5, 1 << 16, 8, oracle)
 
 
 @pytest.mark.parametrize("b", [1 << 16, 1 << 18])

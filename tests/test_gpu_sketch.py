@@ -1,7 +1,7 @@
 """Device-resident sketch object: top-K recovery without the dense estimate
 equals the dense path's top-K exactly (same entries, values and order),
 for one tile and for many small tiles; listed-entry queries equal the dense
-estimate bit for bit."""
+estimate bit for bit; and both against the CPU oracle."""
 import numpy as np
 import pytest
 
@@ -28,6 +28,26 @@ def test_sketch_topk_equals_dense_topk(gpu, variant):
     rng = np.random.default_rng(5)
     qi, qj = rng.integers(0, 700, 500), rng.integers(0, 900, 500)
     np.testing.assert_array_equal(s.entries(qi, qj), C.cpu().numpy()[qi, qj])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant", ["fft", "fwht"])
+def test_sketch_estimates_match_oracle(gpu, oracle, variant):
+    """The device sketch object's listed-entry queries and top-K against the
+    CPU oracle's sketch and median estimates on the same inputs."""
+    import torch
+    AT, B, _ = planted_problem(300, 200, 260, 16, 4321)
+    s = Sketch.compute(torch.from_numpy(AT).cuda(), torch.from_numpy(B).cuda(), 5, 4096, 31, variant)
+    p = oracle.compressed_product(variant, None, AT, B, 5, 4096, 31)
+    want = oracle.decompress(variant, None, p, 5, 4096, 31, 300, 260)
+    rng = np.random.default_rng(9)
+    qi, qj = rng.integers(0, 300, 400), rng.integers(0, 260, 400)
+    np.testing.assert_allclose(s.entries(qi, qj), want[qi, qj], rtol=1e-10,
+                               atol=1e-11 * float(np.abs(want).max()))
+    ti, tj, _ = s.topk(16)
+    from compmatmul_b200.planted import topk_dense_host
+    wi, wj, _ = topk_dense_host(want, 16)
+    assert set(zip(ti.tolist(), tj.tolist())) == set(zip(wi.tolist(), wj.tolist()))
 
 
 @pytest.mark.gpu

@@ -4,8 +4,9 @@ This file is named to be collected last, so that the entry point is also
 exercised after every other test has used the allocating paths.  Each GPU
 case calls the entry twice in a row through the C ABI and compares both
 results with cmm_dev_compressed_product (the allocating entry point) on the
-same device inputs.  Tolerance: 1e-11 * max|p| absolute, as for the sketch
-parity tests (the two entries may sum the k groups in a different order).
+same device inputs, and the second result with the CPU oracle.  Tolerance:
+1e-11 * max|p| absolute, as for the sketch parity tests (the entries may sum
+the k groups in a different order).
 The CPU test checks the size limit, which is enforced before any CUDA call.
 """
 import ctypes as C
@@ -55,7 +56,7 @@ CASES = [
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("variant,h,n_a,n_inner,n_b,d,b,seed", CASES)
-def test_noalloc_matches_allocating_entry(gpu, variant, h, n_a, n_inner, n_b, d, b, seed):
+def test_noalloc_matches_allocating_entry(gpu, oracle, variant, h, n_a, n_inner, n_b, d, b, seed):
     import torch
     L = gpu
     dev = torch.device("cuda:0")
@@ -77,3 +78,6 @@ def test_noalloc_matches_allocating_entry(gpu, variant, h, n_a, n_inner, n_b, d,
         torch.cuda.synchronize()
         np.testing.assert_allclose(p.cpu().numpy(), ref, rtol=0, atol=p_tol(ref),
                                    err_msg=f"call {call + 1}")
+    # and directly against the CPU oracle on the same inputs
+    want = oracle.compressed_product(variant, h, AT.cpu().numpy(), B.cpu().numpy(), d, b, seed)
+    np.testing.assert_allclose(p.cpu().numpy(), want, rtol=0, atol=p_tol(want))
