@@ -304,15 +304,25 @@ static bool try_cluster_plan(int variant, bool f32, const Codes& codes, int64_t 
   // for every FFT case and for FP64 FWHT (167.7 against 176-188 ms per
   // product at b = 2^16); the tensor-core slab kernel wins for FP32 FWHT
   // (513 against 545 ms of sketch kernel at b = 2^18)
-  if (sketch_kernel_choice() == 0 && variant == kVariantFWHT && f32) return false;
-  try {
-    C = plan_cluster(variant, f32, n_inner, sp.d, sp.b, 4096);
-  } catch (const unsupported&) {
-    return false;
+  const bool try_ws = cluster_ws_for(f32);
+  if (sketch_kernel_choice() == 0 && variant == kVariantFWHT && f32 && !try_ws) return false;
+  // the warp-specialized kernels when selected and their segments fit in
+  // shared memory, else the single-group kernels
+  for (int pass = try_ws ? 0 : 1; pass < 2; ++pass) {
+    const bool ws = pass == 0;
+    try {
+      C = plan_cluster(variant, f32, ws, n_inner, sp.d, sp.b, n_a > n_b ? n_a : n_b);
+    } catch (const unsupported&) {
+      if (ws) continue;
+      return false;
+    }
+    plan = make_owner_plan(codes.a.as<uint32_t>(), codes.b.as<uint32_t>(), n_a, n_b, sp.d, sp.b, C.logL,
+                           C.logR2, variant, 9, s);
+    if (cluster_smem_fits(variant, f32, C, plan)) return true;
+    if (!ws) return false;
+    if (variant == kVariantFWHT && f32) return false;  // no single-group FP32 FWHT
   }
-  plan = make_owner_plan(codes.a.as<uint32_t>(), codes.b.as<uint32_t>(), n_a, n_b, sp.d, sp.b, C.logL,
-                         C.logR2, variant, s);
-  return cluster_smem_fits(variant, f32, C, plan);
+  return false;
 }
 
 // Inner indices per cluster-kernel launch: all of them for device inputs;

@@ -477,24 +477,27 @@ namespace cmm {
 // into their first radix pass.  With b = R1 * R2 * L, an index with bucket
 // h belongs to residue class r2 = h mod R2, sub-bucket m = (h mod (b / R1))
 // div R2 (< L) and DIF quotient q1 = h div (b / R1), as for residue plans.
-// The first pass of the CTA's L-point transform is done by kPlanThreads
-// threads, thread j on the QN = L / kPlanThreads points j * QN + e; so
-// thread j owns the sub-buckets those points hold:
-//   FFT  (bit-reversed input): m = brev(j * QN + e) -> j = brev9(m mod 512),
-//        element q = m div 512 (e = brev(q));
+// The first pass of the CTA's L-point transform is done by T = 2^logT
+// threads (512, or 256 in the warp-specialized kernels), thread j on the
+// QN = L / T points j * QN + e; so thread j owns the sub-buckets those
+// points hold:
+//   FFT  (bit-reversed input): m = brev(j * QN + e) -> j = brev_logT(m mod T),
+//        element q = m div T (e = brev(q));
 //   FWHT (natural order):      m = j * QN + e       -> j = m div QN, q = m mod QN.
 // Per (t, side, r2) the members are stably sorted by (owner j, q); thread
 // j's slots are [cut[j], cut[j + 1]).  A slot holds the index (src) and the
 // code q | q1 << 4 | (sign == +1) << 15.
-__device__ __forceinline__ uint32_t owner_key(uint32_t m, int logL, bool fft) {
+// logT = log2 of the threads sharing the first pass (9: 512, 8: 256)
+__device__ __forceinline__ uint32_t owner_key(uint32_t m, int logL, int logT, bool fft) {
   if (!fft) return m;
-  return ((__brev(m & 511u) >> 23) << (logL - 9)) | (m >> 9);
+  const uint32_t tmask = (1u << logT) - 1u;
+  return ((__brev(m & tmask) >> (32 - logT)) << (logL - logT)) | (m >> logT);
 }
 
 __global__ void __launch_bounds__(kSegSortThreads) k_plan_owner_sort(
     const uint32_t* __restrict__ codesA, const uint32_t* __restrict__ codesB, int64_t n_a, int64_t n_b,
-    int logL, int logR2, int logM, int fft, uint32_t* __restrict__ sortedA, uint32_t* __restrict__ sortedB,
-    uint32_t* __restrict__ cut, uint32_t* __restrict__ emax) {
+    int logL, int logR2, int logM, int logT, int fft, uint32_t* __restrict__ sortedA,
+    uint32_t* __restrict__ sortedB, uint32_t* __restrict__ cut, uint32_t* __restrict__ emax) {
   extern __shared__ uint32_t sown[];
   const int L = 1 << logL, R2 = 1 << logR2;
   uint32_t* cnt = sown;
@@ -508,7 +511,7 @@ __global__ void __launch_bounds__(kSegSortThreads) k_plan_owner_sort(
   __syncthreads();
   for (int64_t i = threadIdx.x; i < N; i += kSegSortThreads) {
     const uint32_t h = __ldg(codes + i) & 0x7fffffffu;
-    if ((h & rmask) == (uint32_t)r2) atomicAdd(&cnt[owner_key((h & mmask) >> logR2, logL, fft)], 1u);
+    if ((h & rmask) == (uint32_t)r2) atomicAdd(&cnt[owner_key((h & mmask) >> logR2, logL, logT, fft)], 1u);
   }
   __syncthreads();
   if (threadIdx.x < 32) {  // exclusive scan of cnt[0..L) into cum
@@ -540,7 +543,7 @@ __global__ void __launch_bounds__(kSegSortThreads) k_plan_owner_sort(
     if (valid) {
       const uint32_t h = __ldg(codes + i) & 0x7fffffffu;
       valid = (h & rmask) == (uint32_t)r2;
-      if (valid) key = owner_key((h & mmask) >> logR2, logL, fft);
+      if (valid) key = owner_key((h & mmask) >> logR2, logL, logT, fft);
     }
     const uint32_t peers = __match_any_sync(0xffffffffu, key);
     const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
@@ -551,16 +554,19 @@ __global__ void __launch_bounds__(kSegSortThreads) k_plan_owner_sort(
       __syncthreads();
     }
   }
-  // thread j of the sketch kernel owns keys [j * QN, (j + 1) * QN)
-  const int QB = logL - 9;
+  // thread j of the sketch kernel owns keys [j * QN, (j + 1) * QN); the
+  // cut array keeps kPlanThreads + 1 entries, of which 2^logT + 1 are used
+  const int QB = logL - logT;
   uint32_t* cuts = cut + (((size_t)t * 2 + side) * R2 + r2) * (kPlanThreads + 1);
-  for (int j = threadIdx.x; j <= kPlanThreads; j += kSegSortThreads) cuts[j] = cum[j << QB];
+  for (int j = threadIdx.x; j <= kPlanThreads; j += kSegSortThreads)
+    cuts[j] = j <= (1 << logT) ? cum[j << QB] : cum[L];
   if (threadIdx.x == 0) emax[((size_t)t * 2 + side) * R2 + r2] = cum[L];  // segment size
 }
 
 __global__ void k_plan_owner_layout(const uint32_t* __restrict__ codesA, const uint32_t* __restrict__ codesB,
-                                    int64_t n_a, int64_t n_b, int logL, int logR2, int logM, int fft, int R2,
-                                    const uint32_t* __restrict__ sortedA, const uint32_t* __restrict__ sortedB,
+                                    int64_t n_a, int64_t n_b, int logL, int logR2, int logM, int logT, int fft,
+                                    int R2, const uint32_t* __restrict__ sortedA,
+                                    const uint32_t* __restrict__ sortedB,
                                     const uint32_t* __restrict__ cut, int SA, int SB, uint32_t* __restrict__ srcA,
                                     uint32_t* __restrict__ srcB, uint16_t* __restrict__ codeA,
                                     uint16_t* __restrict__ codeB, uint32_t* __restrict__ cutA,
@@ -575,13 +581,13 @@ __global__ void k_plan_owner_layout(const uint32_t* __restrict__ codesA, const u
   const uint32_t total = cuts[kPlanThreads];
   uint32_t* src = (side == 0 ? srcA : srcB) + ((size_t)t * R2 + r2) * S;
   uint16_t* code = (side == 0 ? codeA : codeB) + ((size_t)t * R2 + r2) * S;
-  const uint32_t mmask = (1u << logM) - 1u, qmask = (1u << (logL - 9)) - 1u;
+  const uint32_t mmask = (1u << logM) - 1u, qmask = (1u << (logL - logT)) - 1u;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < S; e += (int64_t)gridDim.x * blockDim.x) {
     if ((uint32_t)e < total) {
       const uint32_t i = sorted[e];
       const uint32_t c = codes[i];
       const uint32_t h = c & 0x7fffffffu;
-      const uint32_t q = owner_key((h & mmask) >> logR2, logL, fft) & qmask;
+      const uint32_t q = owner_key((h & mmask) >> logR2, logL, logT, fft) & qmask;
       src[e] = i;
       code[e] = (uint16_t)(q | ((h >> logM) << 4) | ((c >> 31) << 15));
     } else {
@@ -595,7 +601,7 @@ __global__ void k_plan_owner_layout(const uint32_t* __restrict__ codesA, const u
 }
 
 SlabPlan make_owner_plan(const uint32_t* dCodesA, const uint32_t* dCodesB, int64_t n_a, int64_t n_b, int d,
-                         int b, int logL, int logR2, int variant, cudaStream_t s) {
+                         int b, int logL, int logR2, int variant, int logT, cudaStream_t s) {
   SlabPlan P;
   P.d = d;
   P.logL = logL;
@@ -605,8 +611,9 @@ SlabPlan make_owner_plan(const uint32_t* dCodesA, const uint32_t* dCodesB, int64
   while ((1 << log2b) < b) ++log2b;
   const int logR1 = log2b - logL - logR2;
   const int logM = log2b - logR1;
-  if (logL < 9 || logL - 9 > 4 || logR1 > 11)
-    throw unsupported("owner plan: slab length or DIF radix out of range");
+  if (logT < 8 || logT > 9 || logL < logT || logL - logT > 4 || logR1 > 11)
+    throw unsupported("owner plan: slab length, first-pass threads or DIF radix out of range");
+  P.owner_logT = logT;
   P.segs = 1 << logR2;
   P.u16 = true;
   P.owner = true;
@@ -620,8 +627,8 @@ SlabPlan make_owner_plan(const uint32_t* dCodesA, const uint32_t* dCodesB, int64
     ProfScope prof("plan", s);
     count_launch();
     k_plan_owner_sort<<<dim3(d, 2, R2), kSegSortThreads, smem, s>>>(
-        dCodesA, dCodesB, n_a, n_b, logL, logR2, logM, fft, sortedA.as<uint32_t>(), sortedB.as<uint32_t>(),
-        cut.as<uint32_t>(), emax.as<uint32_t>());
+        dCodesA, dCodesB, n_a, n_b, logL, logR2, logM, logT, fft, sortedA.as<uint32_t>(),
+        sortedB.as<uint32_t>(), cut.as<uint32_t>(), emax.as<uint32_t>());
     CMM_CUDA(cudaGetLastError());
   }
   // segments hold S slots: the largest segment over (t, r2), rounded to 8
@@ -651,7 +658,7 @@ SlabPlan make_owner_plan(const uint32_t* dCodesA, const uint32_t* dCodesB, int64
   dim3 grid((unsigned)((Smax + 255) / 256 < 256 ? (Smax + 255) / 256 : 256), (unsigned)d, (unsigned)(2 * R2));
   ProfScope prof("plan", s);
   count_launch();
-  k_plan_owner_layout<<<grid, 256, 0, s>>>(dCodesA, dCodesB, n_a, n_b, logL, logR2, logM, fft, R2,
+  k_plan_owner_layout<<<grid, 256, 0, s>>>(dCodesA, dCodesB, n_a, n_b, logL, logR2, logM, logT, fft, R2,
                                            sortedA.as<uint32_t>(), sortedB.as<uint32_t>(), cut.as<uint32_t>(),
                                            (int)SA, (int)SB, P.srcA.as<uint32_t>(), P.srcB.as<uint32_t>(),
                                            P.codeA.as<uint16_t>(), P.codeB.as<uint16_t>(),
