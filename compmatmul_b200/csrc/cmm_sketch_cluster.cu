@@ -84,6 +84,36 @@ __host__ __device__ constexpr int brev_bits(int x) {
   return r;
 }
 
+// Element idx of the same shared array in the CTA of cluster rank `rank`:
+// a 32-bit shared::cluster address from mapa, read with ld.shared::cluster.
+// The loads are volatile, so they stay after the cluster barrier that
+// publishes the data (the barrier is a volatile asm too).
+__device__ __forceinline__ uint32_t cluster_addr(const void* local, int rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n"
+               : "=r"(r)
+               : "r"((uint32_t)__cvta_generic_to_shared(local)), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void ld_cluster(double2& v, uint32_t a) {
+  asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];\n" : "=d"(v.x), "=d"(v.y) : "r"(a));
+}
+__device__ __forceinline__ void ld_cluster(float2& v, uint32_t a) {
+  asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];\n" : "=f"(v.x), "=f"(v.y) : "r"(a));
+}
+__device__ __forceinline__ void ld_cluster(double& v, uint32_t a) {
+  asm volatile("ld.shared::cluster.f64 %0, [%1];\n" : "=d"(v) : "r"(a));
+}
+__device__ __forceinline__ void ld_cluster(float& v, uint32_t a) {
+  asm volatile("ld.shared::cluster.f32 %0, [%1];\n" : "=f"(v) : "r"(a));
+}
+template <typename T>
+__device__ __forceinline__ T remote(const T* local_array, int rank, int idx) {
+  T v;
+  ld_cluster(v, cluster_addr(local_array + idx, rank));
+  return v;
+}
+
 }  // namespace
 
 struct ClArgs {
@@ -573,7 +603,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
         if (R2 == 16) {
           const int rb = half ? 8 : 0;
 #pragma unroll
-          for (int r = 0; r < 8; ++r) z[r] = cluster.map_shared_rank(buf, rb + r)[phys<ES>(n)];
+          for (int r = 0; r < 8; ++r) z[r] = remote(buf, rb + r, phys<ES>(n));
 #pragma unroll
           for (int r = 0; r < 8; ++r) {
             const C o = mk(__shfl_xor_sync(0xffffffffu, z[r].x, 1), __shfl_xor_sync(0xffffffffu, z[r].y, 1));
@@ -583,7 +613,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
           }
         } else {
 #pragma unroll
-          for (int r = 0; r < 8; ++r) z[r] = cluster.map_shared_rank(buf, r)[phys<ES>(n)];
+          for (int r = 0; r < 8; ++r) z[r] = remote(buf, r, phys<ES>(n));
         }
         dft8(z);
 #pragma unroll
@@ -605,8 +635,8 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
           const int rb = half ? 8 : 0;
 #pragma unroll
           for (int r = 0; r < 8; ++r) {
-            zx[r] = cluster.map_shared_rank(xs, rb + r)[phys<ES>(n)];
-            zy[r] = cluster.map_shared_rank(ys, rb + r)[phys<ES>(n)];
+            zx[r] = remote(xs, rb + r, phys<ES>(n));
+            zy[r] = remote(ys, rb + r, phys<ES>(n));
           }
 #pragma unroll
           for (int r = 0; r < 8; ++r) {
@@ -617,8 +647,8 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
         } else {
 #pragma unroll
           for (int r = 0; r < 8; ++r) {
-            zx[r] = cluster.map_shared_rank(xs, r)[phys<ES>(n)];
-            zy[r] = cluster.map_shared_rank(ys, r)[phys<ES>(n)];
+            zx[r] = remote(xs, r, phys<ES>(n));
+            zy[r] = remote(ys, r, phys<ES>(n));
           }
         }
         whtr<Real, 8>(zx);
@@ -796,29 +826,6 @@ __global__ void __launch_bounds__(2 * kWsGroup, 1) k_sketch_cluster_ws(ClArgs a)
   double2* partC = reinterpret_cast<double2*>(a.partial) + ((size_t)g * a.d + t) * (size_t)bsz;
   double* partR = reinterpret_cast<double*>(a.partial) + ((size_t)g * a.d + t) * (size_t)bsz;
   constexpr int QC = kFFT ? 2 : 1;
-  // combine group's accumulators: FP64, or FP32 two-sum pairs
-  double qd[kF32 ? 1 : OUT][QC];
-  float qh[kF32 ? OUT : 1][QC], ql[kF32 ? OUT : 1][QC];
-  if (!sk) {
-#pragma unroll
-    for (int o = 0; o < OUT; ++o) {
-      const int gi = gt + kWsGroup * (o >> 3);
-      double vx = 0.0, vy = 0.0;
-      if (a.accumulate) {
-        const int64_t f = out_f(gi, o & 7);
-        if (kFFT) { const double2 v = partC[f]; vx = v.x; vy = v.y; }
-        else vx = partR[f];
-      }
-      if constexpr (kF32) {
-        qh[o][0] = (float)vx; ql[o][0] = (float)(vx - (double)qh[o][0]);
-        if (kFFT) { qh[o][QC - 1] = (float)vy; ql[o][QC - 1] = (float)(vy - (double)qh[o][QC - 1]); }
-      } else {
-        qd[o][0] = vx;
-        if (kFFT) qd[o][QC - 1] = vy;
-      }
-    }
-  }
-
   const int64_t per = (a.kc + a.G - 1) / a.G;
   const int64_t kb = (int64_t)g * per;
   const int64_t ke = kb + per < a.kc ? kb + per : a.kc;
@@ -850,14 +857,17 @@ __global__ void __launch_bounds__(2 * kWsGroup, 1) k_sketch_cluster_ws(ClArgs a)
   if (sk && kk < ke) stage(kk);
   cluster.sync();  // tables and codes written; the previous item's reads are done
 
-  // iteration: the sketch group transforms kk (if any) into buffer
-  // (step & 1) while the combine group combines the previous index (if
-  // any) from buffer ((step - 1) & 1); one cluster barrier ends both
-  bool have_prev = false;
-  while (kk < ke || have_prev) {
-    const bool have_cur = kk < ke;
-    const int64_t kn = have_cur ? next_k(kk + 1) : kk;
-    if (sk && have_cur) {
+  // The sketch group transforms each inner index into buffer (step & 1);
+  // the combine group combines the previous index from the other buffer.
+  // Iteration i of both loops ends at cluster barrier i: the sketch group
+  // has then written index i and the combine group read index i - 1, so
+  // barrier i publishes the one and retires the reads of the buffer that
+  // index i + 1 overwrites.  Both loops take K + 1 barriers for K indices.
+  // The two groups run separate loops so that the combine group's
+  // accumulators are not live in the sketch group's code.
+  if (sk) {
+    while (kk < ke) {
+      const int64_t kn = next_k(kk + 1);
       Real alpha = (Real)1, beta = (Real)1;
       if (kFFT) {
         const int se = __ldg(a.scale_exp + a.k0 + kk);
@@ -983,8 +993,38 @@ __global__ void __launch_bounds__(2 * kWsGroup, 1) k_sketch_cluster_ws(ClArgs a)
         }
         if (ps < 3) ws_group_sync();
       }
+      cluster.sync();  // sub-spectrum of kk published
+      ++step;
+      kk = kn;
     }
-    if (!sk && have_prev) {
+    cluster.sync();  // the combine group's last index
+  } else {
+    // combine group's accumulators: FP64, or FP32 two-sum pairs
+    double qd[kF32 ? 1 : OUT][QC];
+    float qh[kF32 ? OUT : 1][QC], ql[kF32 ? OUT : 1][QC];
+    {
+#pragma unroll
+      for (int o = 0; o < OUT; ++o) {
+        const int gi = gt + kWsGroup * (o >> 3);
+        double vx = 0.0, vy = 0.0;
+        if (a.accumulate) {
+          const int64_t f = out_f(gi, o & 7);
+          if (kFFT) { const double2 v = partC[f]; vx = v.x; vy = v.y; }
+          else vx = partR[f];
+        }
+        if constexpr (kF32) {
+          qh[o][0] = (float)vx; ql[o][0] = (float)(vx - (double)qh[o][0]);
+          if (kFFT) { qh[o][QC - 1] = (float)vy; ql[o][QC - 1] = (float)(vy - (double)qh[o][QC - 1]); }
+        } else {
+          qd[o][0] = vx;
+          if (kFFT) qd[o][QC - 1] = vy;
+        }
+      }
+    }
+    cluster.sync();  // nothing to combine before the first index
+    while (kk < ke) {
+      const int64_t kn = next_k(kk + 1);
+      ++step;
       const C* buf = buf0 + (size_t)((step - 1) & 1) * PL;
       const Real* xs = xs0 + (size_t)((step - 1) & 1) * 2 * PL;
       const Real* ys = xs + PL;
@@ -999,7 +1039,7 @@ __global__ void __launch_bounds__(2 * kWsGroup, 1) k_sketch_cluster_ws(ClArgs a)
           if (R2 == 16) {
             const int rb = half ? 8 : 0;
 #pragma unroll
-            for (int r = 0; r < 8; ++r) z[r] = cluster.map_shared_rank(buf, rb + r)[phys<ES>(n)];
+            for (int r = 0; r < 8; ++r) z[r] = remote(buf, rb + r, phys<ES>(n));
 #pragma unroll
             for (int r = 0; r < 8; ++r) {
               const C o = mk(__shfl_xor_sync(0xffffffffu, z[r].x, 1), __shfl_xor_sync(0xffffffffu, z[r].y, 1));
@@ -1008,7 +1048,7 @@ __global__ void __launch_bounds__(2 * kWsGroup, 1) k_sketch_cluster_ws(ClArgs a)
             }
           } else {
 #pragma unroll
-            for (int r = 0; r < 8; ++r) z[r] = cluster.map_shared_rank(buf, r)[phys<ES>(n)];
+            for (int r = 0; r < 8; ++r) z[r] = remote(buf, r, phys<ES>(n));
           }
           dft8(z);
 #pragma unroll
@@ -1030,8 +1070,8 @@ __global__ void __launch_bounds__(2 * kWsGroup, 1) k_sketch_cluster_ws(ClArgs a)
             const int rb = half ? 8 : 0;
 #pragma unroll
             for (int r = 0; r < 8; ++r) {
-              zx[r] = cluster.map_shared_rank(xs, rb + r)[phys<ES>(n)];
-              zy[r] = cluster.map_shared_rank(ys, rb + r)[phys<ES>(n)];
+              zx[r] = remote(xs, rb + r, phys<ES>(n));
+              zy[r] = remote(ys, rb + r, phys<ES>(n));
             }
 #pragma unroll
             for (int r = 0; r < 8; ++r) {
@@ -1042,8 +1082,8 @@ __global__ void __launch_bounds__(2 * kWsGroup, 1) k_sketch_cluster_ws(ClArgs a)
           } else {
 #pragma unroll
             for (int r = 0; r < 8; ++r) {
-              zx[r] = cluster.map_shared_rank(xs, r)[phys<ES>(n)];
-              zy[r] = cluster.map_shared_rank(ys, r)[phys<ES>(n)];
+              zx[r] = remote(xs, r, phys<ES>(n));
+              zy[r] = remote(ys, r, phys<ES>(n));
             }
           }
           whtr<Real, 8>(zx);
@@ -1055,32 +1095,28 @@ __global__ void __launch_bounds__(2 * kWsGroup, 1) k_sketch_cluster_ws(ClArgs a)
           }
         }
       }
-    }
-    cluster.sync();  // new sub-spectra published; reads of the other buffer retired
-    have_prev = have_cur;
-    if (have_cur) {
-      ++step;
+      cluster.sync();  // reads of buffer (step - 1) & 1 retired
       kk = kn;
+    }
+    {
+#pragma unroll
+      for (int o = 0; o < OUT; ++o) {
+        const int gi = gt + kWsGroup * (o >> 3);
+        const int64_t f = out_f(gi, o & 7);
+        double vx, vy;
+        if constexpr (kF32) {
+          vx = (double)qh[o][0] + (double)ql[o][0];
+          vy = (double)qh[o][QC - 1] + (double)ql[o][QC - 1];
+        } else {
+          vx = qd[o][0];
+          vy = qd[o][QC - 1];
+        }
+        if (kFFT) partC[f] = make_double2(vx, vy);
+        else partR[f] = vx;
+      }
     }
   }
 
-  if (!sk) {
-#pragma unroll
-    for (int o = 0; o < OUT; ++o) {
-      const int gi = gt + kWsGroup * (o >> 3);
-      const int64_t f = out_f(gi, o & 7);
-      double vx, vy;
-      if constexpr (kF32) {
-        vx = (double)qh[o][0] + (double)ql[o][0];
-        vy = (double)qh[o][QC - 1] + (double)ql[o][QC - 1];
-      } else {
-        vx = qd[o][0];
-        vy = qd[o][QC - 1];
-      }
-      if (kFFT) partC[f] = make_double2(vx, vy);
-      else partR[f] = vx;
-    }
-  }
   }  // item loop
 }
 
