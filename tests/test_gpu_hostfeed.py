@@ -7,9 +7,10 @@ kernels' own chunking (an eighth of the inner range per launch) the
 products below run several chunks through that feed, on every sketch kernel
 family.  Each launch splits its own chunk into k-groups, so the host path
 sums the inner indices in a different grouping than the single launch of
-the device entry point: the two agree within 1e-13 * max|p| (bit-identical
-when both run one launch), and both are within the usual tolerance of the
-oracle: FP64 sketch within 1e-11 * max|p|, mixed within 2e-5 * max|p|.
+the device entry point: the two agree within 1e-13 * max|p| (FP64) or
+1e-7 * max|p| (mixed; bit-identical when both run one launch), and both are
+within the usual tolerance of the oracle: FP64 sketch within 1e-11 * max|p|,
+mixed within 2e-5 * max|p|.
 """
 import numpy as np
 import pytest
@@ -40,7 +41,9 @@ def test_streamed_rows_match_device_path(gpu, oracle, variant, b, f32, monkeypat
     kern = lib().cmm_last_sketch_kernel().decode()
     p_dev = device.compressed_product(torch.from_numpy(AT).cuda(), torch.from_numpy(B).cuda(), d, b, seed,
                                       variant).cpu().numpy()
-    np.testing.assert_allclose(p_host, p_dev, rtol=0, atol=1e-13 * float(np.abs(p_dev).max()), err_msg=kern)
+    # FP32 transforms round each grouping's partial sums differently
+    agree = 1e-7 if f32 else 1e-13
+    np.testing.assert_allclose(p_host, p_dev, rtol=0, atol=agree * float(np.abs(p_dev).max()), err_msg=kern)
     ref = oracle.compressed_product(variant, None, AT.astype(np.float64), B.astype(np.float64), d, b, seed)
     tol = 2e-5 if f32 else 1e-11
     np.testing.assert_allclose(p_host, ref, rtol=0, atol=tol * float(np.abs(ref).max()), err_msg=kern)
