@@ -477,17 +477,18 @@ namespace cmm {
 // into their first radix pass.  With b = R1 * R2 * L, an index with bucket
 // h belongs to residue class r2 = h mod R2, sub-bucket m = (h mod (b / R1))
 // div R2 (< L) and DIF quotient q1 = h div (b / R1), as for residue plans.
-// The first pass of the CTA's L-point transform is done by T = 2^logT
-// threads (512, or 256 in the warp-specialized kernels), thread j on the
-// QN = L / T points j * QN + e; so thread j owns the sub-buckets those
-// points hold:
+// The first pass of the CTA's L-point transform is done by T = 2^logT = 512
+// threads, thread j on the QN = L / T points j * QN + e; so thread j owns
+// the sub-buckets those points hold:
 //   FFT  (bit-reversed input): m = brev(j * QN + e) -> j = brev_logT(m mod T),
 //        element q = m div T (e = brev(q));
 //   FWHT (natural order):      m = j * QN + e       -> j = m div QN, q = m mod QN.
 // Per (t, side, r2) the members are stably sorted by (owner j, q); thread
-// j's slots are [cut[j], cut[j + 1]).  A slot holds the index (src) and the
-// code q | q1 << 4 | (sign == +1) << 15.
-// logT = log2 of the threads sharing the first pass (9: 512, 8: 256)
+// j's slots are [cut[j], cut[j + 1]).  A slot holds src = index |
+// (sign == +1) << 31 (kPadSlot past the segment's end, as the residue plans,
+// so k_materialize can copy the rows in slot order) and the code
+// q | q1 << 4 | (sign == +1) << 15.
+// logT = log2 of the threads sharing the first pass
 __device__ __forceinline__ uint32_t owner_key(uint32_t m, int logL, int logT, bool fft) {
   if (!fft) return m;
   const uint32_t tmask = (1u << logT) - 1u;
@@ -554,8 +555,7 @@ __global__ void __launch_bounds__(kSegSortThreads) k_plan_owner_sort(
       __syncthreads();
     }
   }
-  // thread j of the sketch kernel owns keys [j * QN, (j + 1) * QN); the
-  // cut array keeps kPlanThreads + 1 entries, of which 2^logT + 1 are used
+  // thread j of the sketch kernel owns keys [j * QN, (j + 1) * QN)
   const int QB = logL - logT;
   uint32_t* cuts = cut + (((size_t)t * 2 + side) * R2 + r2) * (kPlanThreads + 1);
   for (int j = threadIdx.x; j <= kPlanThreads; j += kSegSortThreads)
@@ -588,10 +588,10 @@ __global__ void k_plan_owner_layout(const uint32_t* __restrict__ codesA, const u
       const uint32_t c = codes[i];
       const uint32_t h = c & 0x7fffffffu;
       const uint32_t q = owner_key((h & mmask) >> logR2, logL, logT, fft) & qmask;
-      src[e] = i;
+      src[e] = i | (c & 0x80000000u);
       code[e] = (uint16_t)(q | ((h >> logM) << 4) | ((c >> 31) << 15));
     } else {
-      src[e] = 0;
+      src[e] = kPadSlot;
       code[e] = 0;
     }
   }
@@ -601,7 +601,8 @@ __global__ void k_plan_owner_layout(const uint32_t* __restrict__ codesA, const u
 }
 
 SlabPlan make_owner_plan(const uint32_t* dCodesA, const uint32_t* dCodesB, int64_t n_a, int64_t n_b, int d,
-                         int b, int logL, int logR2, int variant, int logT, cudaStream_t s) {
+                         int b, int logL, int logR2, int variant, cudaStream_t s) {
+  const int logT = 9;  // the cluster kernels' kPlanThreads first-pass threads
   SlabPlan P;
   P.d = d;
   P.logL = logL;
@@ -611,9 +612,8 @@ SlabPlan make_owner_plan(const uint32_t* dCodesA, const uint32_t* dCodesB, int64
   while ((1 << log2b) < b) ++log2b;
   const int logR1 = log2b - logL - logR2;
   const int logM = log2b - logR1;
-  if (logT < 8 || logT > 9 || logL < logT || logL - logT > 4 || logR1 > 11)
-    throw unsupported("owner plan: slab length, first-pass threads or DIF radix out of range");
-  P.owner_logT = logT;
+  if (logL < logT || logL - logT > 4 || logR1 > 11)
+    throw unsupported("owner plan: slab length or DIF radix out of range");
   P.segs = 1 << logR2;
   P.u16 = true;
   P.owner = true;

@@ -15,11 +15,13 @@
 //    frequencies of L / R2 sub-spectrum positions and accumulates
 //    Z^2 (FFT, z = alpha x + i beta y) or X * Y (FWHT) for them over k.
 //
-// Inputs are read straight from the rows of AT and B (row k of AT is column
-// k of A): per inner index the CTA gathers the values of its residue segment
-// with cp.async (the plan lists their indices), one row ahead of the one it
-// transforms.  A row is read from HBM about once and then from L2 by the
-// R1 * d items that need it; there are no per-repetition copies of the rows.
+// Rows reach the staging area in one of two ways, both in the plan's slot
+// order, one row ahead of the one being transformed: copied contiguously
+// from per-chunk copies of the rows (k_materialize writes each repetition's
+// segments with the sign applied), or gathered from the rows of AT and B
+// in place with cp.async, one 8-byte (or 4-byte) load per slot.  The copy
+// is the default: on B200 the gathers of a config-2 product (about 10^10
+// scattered 8-byte loads) cost more than writing and re-reading the copies.
 //
 // The count sketch is fused into the first radix pass: the owner plan
 // (cmm_plan.cu) sorts a segment by the thread whose first butterfly reads
@@ -119,8 +121,10 @@ __device__ __forceinline__ T remote(const T* local_array, int rank, int idx) {
 struct ClArgs {
   const void* A;          // AT (n_inner x lda), row k at A + k * lda
   const void* B;          // B (n_inner x ldb)
+  const void* matA;       // or NULL: rows k0 .. k0 + kc copied in slot order, sign applied,
+  const void* matB;       //   [t][kk][R2][SA] (then A / B are not read)
   int64_t lda, ldb;
-  const uint32_t* srcA;   // [t][R2][SA] index of each slot
+  const uint32_t* srcA;   // [t][R2][SA] index | (sign == +1) << 31 of each slot
   const uint32_t* srcB;
   const uint16_t* codeA;  // [t][R2][SA] q | q1 << 4 | (sign == +1) << 15
   const uint16_t* codeB;
@@ -371,15 +375,29 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
       for (int u = 0; u < 4; ++u) {
         const int e = e0 + u * kCT;
         if (e < tot) {
-          if (kF32) cp_async4(st + spad<Real>(e), row + ix[u]);
-          else cp_async8(st + spad<Real>(e), row + ix[u]);
+          if (kF32) cp_async4(st + spad<Real>(e), row + (ix[u] & 0x7fffffffu));
+          else cp_async8(st + spad<Real>(e), row + (ix[u] & 0x7fffffffu));
         }
       }
     }
   };
+  // copied rows: this CTA's segments of row k are contiguous (thread i
+  // copies slots i, i + 512, ...)
+  auto copy = [&](const Real* seg, Real* st, int tot) {
+    for (int e = tid; e < tot; e += kCT) {
+      if (kF32) cp_async4(st + spad<Real>(e), seg + e);
+      else cp_async8(st + spad<Real>(e), seg + e);
+    }
+  };
+  const bool copied = a.matA != nullptr;
   auto stage = [&](int64_t k) {
-    gather(reinterpret_cast<const Real*>(a.A) + (size_t)(a.k0 + k) * (size_t)a.lda, srcA, stA, totA);
-    gather(reinterpret_cast<const Real*>(a.B) + (size_t)(a.k0 + k) * (size_t)a.ldb, srcB, stB, totB);
+    if (copied) {
+      copy(reinterpret_cast<const Real*>(a.matA) + (((size_t)t * a.kc + k) * R2 + r2) * a.SA, stA, totA);
+      copy(reinterpret_cast<const Real*>(a.matB) + (((size_t)t * a.kc + k) * R2 + r2) * a.SB, stB, totB);
+    } else {
+      gather(reinterpret_cast<const Real*>(a.A) + (size_t)(a.k0 + k) * (size_t)a.lda, srcA, stA, totA);
+      gather(reinterpret_cast<const Real*>(a.B) + (size_t)(a.k0 + k) * (size_t)a.ldb, srcB, stB, totB);
+    }
   };
   int64_t kk = next_k(kb);
   if (kk < ke) stage(kk);
@@ -425,7 +443,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
       for (int q = 0; q < QN; ++q) {
         while (s < end && (int)(c & 15u) == q) {
           Real v = st[spad<Real>(s)] * sc;
-          if (!(c >> 15)) v = -v;
+          if (!copied && !(c >> 15)) v = -v;  // copied rows carry their sign
           const uint32_t w = (c >> 4) & 0x7ffu;
           if constexpr (!kFFT) {
             if (w) v = -v;
@@ -678,479 +696,26 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
   if (NB == 2) cluster.sync();  // the other CTAs' last reads of this CTA's buffers
 }
 
-// ------------------------------------------- warp-specialized FP64 kernel
-// The same computation for the plain (FP64) path with L = 4096 for both
-// variants, split between two warp groups of one CTA:
-//  * warps 0-7 (the sketch group) gather row k, sum the count sketch into
-//    registers (the 512-owner plan, two owners of 8 points per thread), run
-//    the local transform (four radix-8 passes) and write the sub-spectrum
-//    into buffer (step & 1);
-//  * warps 8-15 (the combine group) meanwhile combine the sub-spectra of
-//    the previous inner index from the other buffer across the cluster and
-//    accumulate its outputs.
-// One cluster barrier per inner index ends both: it publishes the new
-// sub-spectra and retires every CTA's reads of the buffer written next, so
-// the DSMEM-bound combine overlaps the shared-memory-bound transform.  The
-// sketch group's internal barriers are a named barrier of its 256 threads.
-// Both groups take the same k sequence and the same number of cluster
-// barriers (one per index, plus one that drains the last combine).
-namespace {
-constexpr int kWsGroup = 256;  // threads per warp group
-
-__device__ __forceinline__ void ws_group_sync() { asm volatile("bar.sync 1, 256;\n" ::: "memory"); }
-}  // namespace
-
-__host__ __device__ inline ClLayout ws_layout(bool fft, bool f32, int R1, int log2b, int64_t SA, int64_t SB) {
-  const size_t L = 4096, real = f32 ? 4 : 8, cpx = 2 * real;
-  auto plen = [](size_t n, size_t es) { return es == 4 ? n + n / 32 : n + n / 16; };
-  ClLayout o;
-  size_t p = 0;
-  o.buf = p;
-  p += 2 * (fft ? plen(L, cpx) * cpx : 2 * plen(L, real) * real);
-  o.post = p;
-  if (fft) p += (128 + 32) * cpx;
-  o.pre = p;
-  if (fft && R1 > 1) p += (cl_pre_hi(log2b) + 512) * cpx;
-  o.ptw = p;
-  if (fft) p += 592 * cpx;
-  o.wr = p;
-  p += 32 * real;
-  o.stage = p;
-  p += cl_align16((size_t)(spad_len_n(SA, real) + spad_len_n(SB, real)) * real);
-  o.codes = p;
-  p += cl_align16((size_t)(SA + SB) * 2);
-  o.total = p;
-  return o;
-}
-
-template <int VARIANT, typename Real>
-__global__ void __launch_bounds__(2 * kWsGroup, 1) k_sketch_cluster_ws(ClArgs a) {
-  constexpr bool kFFT = VARIANT == kVariantFFT;
-  constexpr bool kF32 = sizeof(Real) == 4;
-  constexpr int LOGL = 12;
-  constexpr int L = 1 << LOGL;
-  using C = typename std::conditional<kF32, float2, double2>::type;
-  constexpr int ES = kFFT ? (int)sizeof(C) : (int)sizeof(Real);
-  constexpr int PL = phys_len<ES>(L);
-  constexpr int OUT = L / kWsGroup;  // 16 outputs per combine thread
-
-  extern __shared__ __align__(16) unsigned char sm[];
-  cg::cluster_group cluster = cg::this_cluster();
-  const int tid = threadIdx.x;
-  const bool sk = tid < kWsGroup;  // sketch group; else combine group
-  const int gt = sk ? tid : tid - kWsGroup;
-  const int R1 = 1 << a.logR1, R2 = 1 << a.logR2;
-  const int r2 = (int)cluster.block_rank();
-  const int logM = a.log2b - a.logR1;
-  const double2* tw = a.tw;
-
-  const ClLayout lay = ws_layout(kFFT, kF32, R1, a.log2b, a.SA, a.SB);
-  C* buf0 = reinterpret_cast<C*>(sm + lay.buf);
-  Real* xs0 = reinterpret_cast<Real*>(sm + lay.buf);
-  C* postLo = reinterpret_cast<C*>(sm + lay.post);  // w_M^{n r2} = postHi[n >> 7] postLo[n & 127]
-  C* postHi = postLo + 128;
-  C* preHi = reinterpret_cast<C*>(sm + lay.pre);
-  C* preLo = preHi + cl_pre_hi(a.log2b);
-  C* ptw = reinterpret_cast<C*>(sm + lay.ptw);  // [0,8) w_64, [8,72) w_512, [72,584) w_4096, [584,592) w_16
-  Real* wRx = reinterpret_cast<Real*>(sm + lay.wr);
-  Real* wRy = wRx + 16;
-  Real* stA = reinterpret_cast<Real*>(sm + lay.stage);
-  Real* stB = stA + spad_len<Real>(a.SA);
-  uint16_t* cA = reinterpret_cast<uint16_t*>(sm + lay.codes);
-  uint16_t* cB = cA + a.SA;
-
-  if (kFFT) {
-    for (int e = tid; e < 128 + 32; e += 2 * kWsGroup) {
-      const uint64_t n = e < 128 ? (uint64_t)e : (uint64_t)(e - 128) << 7;
-      const double2 w = tw[(n * (uint64_t)r2) << a.logR1];
-      postLo[e] = mk((Real)w.x, (Real)w.y);
-    }
-    if (R1 > 1) {
-      for (int e = tid; e < cl_pre_hi(a.log2b); e += 2 * kWsGroup) {
-        const uint64_t x = (uint64_t)e << 9;
-        const double2 w = x < ((uint64_t)1 << a.log2b) ? tw[x] : make_double2(1.0, 0.0);
-        preHi[e] = mk((Real)w.x, (Real)w.y);
-      }
-      for (int e = tid; e < 512; e += 2 * kWsGroup) preLo[e] = mk((Real)tw[e].x, (Real)tw[e].y);
-    }
-    for (int e = tid; e < 8 + 64 + 512 + 8; e += 2 * kWsGroup) {
-      const int lg = e < 8 ? 6 : (e < 72 ? 9 : (e < 584 ? 12 : 4));
-      const int kk = e < 8 ? e : (e < 72 ? e - 8 : (e < 584 ? e - 72 : e - 584));
-      const double2 w = tw[(uint32_t)kk << (a.log2b - lg)];
-      ptw[e] = mk((Real)w.x, (Real)w.y);
-    }
-    for (int e = tid; e < 16; e += 2 * kWsGroup) {
-      const double2 w = e < R1 ? tw[(uint32_t)e << logM] : make_double2(1.0, 0.0);
-      wRx[e] = (Real)w.x;
-      wRy[e] = (Real)w.y;
-    }
-  }
-  auto post = [&](int n) -> C { return cmul(postHi[n >> 7], postLo[n & 127]); };
-
-  unsigned step = 0;
-  const int items = (R1 * a.d) * a.G;
-  for (int item = blockIdx.y; item < items; item += gridDim.y) {
-  const int r1 = item & (R1 - 1);
-  const int t = (item >> a.logR1) % a.d;
-  const int g = (item >> a.logR1) / a.d;
-  __syncthreads();  // the previous item is done with the shared codes and staged rows
-  {
-    const uint16_t* gA = a.codeA + ((size_t)t * R2 + r2) * a.SA;
-    const uint16_t* gB = a.codeB + ((size_t)t * R2 + r2) * a.SB;
-    for (int64_t e = tid; e < a.SA + a.SB; e += 2 * kWsGroup) {
-      const uint32_t c = e < a.SA ? (uint32_t)gA[e] : (uint32_t)gB[e - a.SA];
-      const uint32_t q1 = (c >> 4) & 0x7ffu;
-      const uint32_t w = kFFT ? ((q1 * (uint32_t)r1) & (uint32_t)(R1 - 1)) : (__popc(q1 & (uint32_t)r1) & 1u);
-      (e < a.SA ? cA[e] : cB[e - a.SA]) = (uint16_t)((c & 0x800fu) | (w << 4));
-    }
-  }
-  const uint32_t* cutA = a.cutA + ((size_t)t * R2 + r2) * (kCT + 1);
-  const uint32_t* cutB = a.cutB + ((size_t)t * R2 + r2) * (kCT + 1);
-  const uint32_t* srcA = a.srcA + ((size_t)t * R2 + r2) * a.SA;
-  const uint32_t* srcB = a.srcB + ((size_t)t * R2 + r2) * a.SB;
-  const int totA = (int)cutA[kCT], totB = (int)cutB[kCT];
-
-  const int64_t bsz = (int64_t)1 << a.log2b;
-  auto out_f = [&](int gi, int jj) -> int64_t {
-    const int nl = gi >> (a.logR2 - 3);
-    const int half = gi & ((R2 >> 3) - 1);
-    const int n = r2 * (L >> a.logR2) + nl;
-    if (kFFT) {
-      const int j = R2 == 16 ? 2 * jj + half : jj;
-      return ((int64_t)n + (int64_t)L * j) * R1 + r1;
-    } else {
-      const int j = R2 == 16 ? half * 8 + jj : jj;
-      return (int64_t)r1 * (bsz >> a.logR1) + (int64_t)n * R2 + j;
-    }
-  };
-  double2* partC = reinterpret_cast<double2*>(a.partial) + ((size_t)g * a.d + t) * (size_t)bsz;
-  double* partR = reinterpret_cast<double*>(a.partial) + ((size_t)g * a.d + t) * (size_t)bsz;
-  constexpr int QC = kFFT ? 2 : 1;
-  const int64_t per = (a.kc + a.G - 1) / a.G;
-  const int64_t kb = (int64_t)g * per;
-  const int64_t ke = kb + per < a.kc ? kb + per : a.kc;
-  auto next_k = [&](int64_t k) -> int64_t {
-    if (kFFT)
-      while (k < ke && __ldg(a.scale_exp + a.k0 + k) == kCSkip) ++k;
-    return k;
-  };
-  auto gather = [&](const Real* row, const uint32_t* src, Real* st, int tot) {
-    for (int e0 = gt; e0 < tot; e0 += 4 * kWsGroup) {
-      uint32_t ix[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) ix[u] = e0 + u * kWsGroup < tot ? __ldg(src + e0 + u * kWsGroup) : 0u;
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int e = e0 + u * kWsGroup;
-        if (e < tot) {
-          if (kF32) cp_async4(st + spad<Real>(e), row + ix[u]);
-          else cp_async8(st + spad<Real>(e), row + ix[u]);
-        }
-      }
-    }
-  };
-  auto stage = [&](int64_t k) {
-    gather(reinterpret_cast<const Real*>(a.A) + (size_t)(a.k0 + k) * (size_t)a.lda, srcA, stA, totA);
-    gather(reinterpret_cast<const Real*>(a.B) + (size_t)(a.k0 + k) * (size_t)a.ldb, srcB, stB, totB);
-  };
-  int64_t kk = next_k(kb);
-  if (sk && kk < ke) stage(kk);
-  cluster.sync();  // tables and codes written; the previous item's reads are done
-
-  // The sketch group transforms each inner index into buffer (step & 1);
-  // the combine group combines the previous index from the other buffer.
-  // Iteration i of both loops ends at cluster barrier i: the sketch group
-  // has then written index i and the combine group read index i - 1, so
-  // barrier i publishes the one and retires the reads of the buffer that
-  // index i + 1 overwrites.  Both loops take K + 1 barriers for K indices.
-  // The two groups run separate loops so that the combine group's
-  // accumulators are not live in the sketch group's code.
-  if (sk) {
-    while (kk < ke) {
-      const int64_t kn = next_k(kk + 1);
-      Real alpha = (Real)1, beta = (Real)1;
-      if (kFFT) {
-        const int se = __ldg(a.scale_exp + a.k0 + kk);
-        alpha = kF32 ? (Real)__int_as_float((127 - se) << 23) : (Real)__longlong_as_double((long long)(1023 - se) << 52);
-        beta = kF32 ? (Real)__int_as_float((127 + se) << 23) : (Real)__longlong_as_double((long long)(1023 + se) << 52);
-      }
-      C* buf = buf0 + (size_t)(step & 1) * PL;
-      Real* xs = xs0 + (size_t)(step & 1) * 2 * PL;
-      Real* ys = xs + PL;
-      cp_async_wait_all();
-      ws_group_sync();  // the sketch group's copies of row kk are visible
-      // first pass: each sketch thread takes the 8-point butterflies of
-      // owners gt and gt + 256 of the 512-owner plan (points j * 8 + e),
-      // summing each owner's slots into registers first
-#pragma unroll 1
-      for (int h = 0; h < 2; ++h) {
-        const int j = gt + kWsGroup * h;
-        C acc[8];
-        Real ya[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          acc[q] = mk((Real)0, (Real)0);
-          ya[q] = (Real)0;
-        }
-#pragma unroll
-        for (int side = 0; side < 2; ++side) {
-          const Real* st = side == 0 ? stA : stB;
-          const uint16_t* codes = side == 0 ? cA : cB;
-          const uint32_t* cut = side == 0 ? cutA : cutB;
-          const int end = (int)cut[j + 1];
-          const Real sc = side == 0 ? alpha : beta;
-          int s = (int)cut[j];
-          uint32_t c = s < end ? (uint32_t)codes[s] : 0u;
-#pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            while (s < end && (int)(c & 15u) == q) {
-              Real v = st[spad<Real>(s)] * sc;
-              if (!(c >> 15)) v = -v;
-              const uint32_t w = (c >> 4) & 0x7ffu;
-              if constexpr (!kFFT) {
-                if (w) v = -v;
-                if (side == 0) acc[q].x += v;
-                else ya[q] += v;
-              } else if (a.logR1 <= 1) {
-                if (w & 1u) v = -v;
-                if (side == 0) acc[q].x += v;
-                else acc[q].y += v;
-              } else {
-                Real cx, cy;
-                if (a.logR1 == 2) {
-                  cx = (w & 1u) ? (Real)0 : ((w & 2u) ? -v : v);
-                  cy = (w & 1u) ? ((w & 2u) ? v : -v) : (Real)0;
-                } else {
-                  cx = v * wRx[w];
-                  cy = v * wRy[w];
-                }
-                if (side == 0) acc[q] = mk(acc[q].x + cx, acc[q].y + cy);
-                else acc[q] = mk(acc[q].x - cy, acc[q].y + cx);
-              }
-              ++s;
-              c = s < end ? (uint32_t)codes[s] : 0u;
-            }
-          }
-        }
-        const int base = j * 8;
-        if constexpr (kFFT) {
-          C x[8];
-#pragma unroll
-          for (int e = 0; e < 8; ++e) x[e] = acc[brev_bits<3>(e)];
-          if (R1 > 1) {
-#pragma unroll
-            for (int e = 0; e < 8; ++e) {
-              const uint32_t m = __brev((uint32_t)(base + e)) >> (32 - LOGL);
-              const uint32_t xx = ((m << a.logR2) + (uint32_t)r2) * (uint32_t)r1;
-              x[e] = cmul(x[e], cmul(preHi[xx >> 9], preLo[xx & 511]));
-            }
-          }
-          r8_first(x);
-#pragma unroll
-          for (int e = 0; e < 8; ++e) buf[phys<ES>(base + e)] = x[e];
-        } else {
-          Real x[8], y[8];
-#pragma unroll
-          for (int e = 0; e < 8; ++e) { x[e] = acc[e].x; y[e] = ya[e]; }
-          whtr<Real, 8>(x);
-          whtr<Real, 8>(y);
-#pragma unroll
-          for (int e = 0; e < 8; ++e) { xs[phys<ES>(base + e)] = x[e]; ys[phys<ES>(base + e)] = y[e]; }
-        }
-      }
-      ws_group_sync();  // staged row free; pass 0 written
-      if (kn < ke) stage(kn);
-      // three radix-8 passes, two butterflies per sketch thread; the FFT's
-      // last one applies the post-twiddle w_M^{n r2}
-#pragma unroll
-      for (int ps = 1; ps < 4; ++ps) {
-        const int s0 = 3 * ps, half = 1 << s0;
-#pragma unroll
-        for (int gg = 0; gg < 2; ++gg) {
-          const int gi = gt + gg * kWsGroup;
-          const int kk2 = gi & (half - 1);
-          const int base = ((gi >> s0) << (s0 + 3)) | kk2;
-          if constexpr (kFFT) {
-            C x[8];
-#pragma unroll
-            for (int e = 0; e < 8; ++e) x[e] = buf[phys<ES>(base + e * half)];
-            r8(x, ptw[(ps == 1 ? 0 : (ps == 2 ? 8 : 72)) + kk2]);
-            if (ps == 3) {
-#pragma unroll
-              for (int e = 0; e < 8; ++e) x[e] = cmul(x[e], post(base + e * half));
-            }
-#pragma unroll
-            for (int e = 0; e < 8; ++e) buf[phys<ES>(base + e * half)] = x[e];
-          } else {
-            Real x[8], y[8];
-#pragma unroll
-            for (int e = 0; e < 8; ++e) { x[e] = xs[phys<ES>(base + e * half)]; y[e] = ys[phys<ES>(base + e * half)]; }
-            whtr<Real, 8>(x);
-            whtr<Real, 8>(y);
-#pragma unroll
-            for (int e = 0; e < 8; ++e) { xs[phys<ES>(base + e * half)] = x[e]; ys[phys<ES>(base + e * half)] = y[e]; }
-          }
-        }
-        if (ps < 3) ws_group_sync();
-      }
-      cluster.sync();  // sub-spectrum of kk published
-      ++step;
-      kk = kn;
-    }
-    cluster.sync();  // the combine group's last index
-  } else {
-    // combine group's accumulators: FP64, or FP32 two-sum pairs
-    double qd[kF32 ? 1 : OUT][QC];
-    float qh[kF32 ? OUT : 1][QC], ql[kF32 ? OUT : 1][QC];
-    {
-#pragma unroll
-      for (int o = 0; o < OUT; ++o) {
-        const int gi = gt + kWsGroup * (o >> 3);
-        double vx = 0.0, vy = 0.0;
-        if (a.accumulate) {
-          const int64_t f = out_f(gi, o & 7);
-          if (kFFT) { const double2 v = partC[f]; vx = v.x; vy = v.y; }
-          else vx = partR[f];
-        }
-        if constexpr (kF32) {
-          qh[o][0] = (float)vx; ql[o][0] = (float)(vx - (double)qh[o][0]);
-          if (kFFT) { qh[o][QC - 1] = (float)vy; ql[o][QC - 1] = (float)(vy - (double)qh[o][QC - 1]); }
-        } else {
-          qd[o][0] = vx;
-          if (kFFT) qd[o][QC - 1] = vy;
-        }
-      }
-    }
-    cluster.sync();  // nothing to combine before the first index
-    while (kk < ke) {
-      const int64_t kn = next_k(kk + 1);
-      ++step;
-      const C* buf = buf0 + (size_t)((step - 1) & 1) * PL;
-      const Real* xs = xs0 + (size_t)((step - 1) & 1) * 2 * PL;
-      const Real* ys = xs + PL;
-#pragma unroll
-      for (int u = 0; u < OUT / 8; ++u) {
-        const int gi = gt + kWsGroup * u;
-        const int nl = gi >> (a.logR2 - 3);
-        const int half = gi & ((R2 >> 3) - 1);
-        const int n = r2 * (L >> a.logR2) + nl;
-        if (kFFT) {
-          C z[8];
-          if (R2 == 16) {
-            const int rb = half ? 8 : 0;
-#pragma unroll
-            for (int r = 0; r < 8; ++r) z[r] = remote(buf, rb + r, phys<ES>(n));
-#pragma unroll
-            for (int r = 0; r < 8; ++r) {
-              const C o = mk(__shfl_xor_sync(0xffffffffu, z[r].x, 1), __shfl_xor_sync(0xffffffffu, z[r].y, 1));
-              if (half == 0) z[r] = mk(z[r].x + o.x, z[r].y + o.y);
-              else z[r] = cmul(mk(o.x - z[r].x, o.y - z[r].y), ptw[584 + r]);
-            }
-          } else {
-#pragma unroll
-            for (int r = 0; r < 8; ++r) z[r] = remote(buf, r, phys<ES>(n));
-          }
-          dft8(z);
-#pragma unroll
-          for (int jj = 0; jj < 8; ++jj) {
-            const int o = u * 8 + jj;
-            const Real zr = z[jj].x * z[jj].x - z[jj].y * z[jj].y;
-            const Real zi = (z[jj].x + z[jj].x) * z[jj].y;
-            if constexpr (kF32) {
-              tsum(qh[o][0], ql[o][0], zr);
-              tsum(qh[o][QC - 1], ql[o][QC - 1], zi);
-            } else {
-              qd[o][0] += zr;
-              qd[o][QC - 1] += zi;
-            }
-          }
-        } else {
-          Real zx[8], zy[8];
-          if (R2 == 16) {
-            const int rb = half ? 8 : 0;
-#pragma unroll
-            for (int r = 0; r < 8; ++r) {
-              zx[r] = remote(xs, rb + r, phys<ES>(n));
-              zy[r] = remote(ys, rb + r, phys<ES>(n));
-            }
-#pragma unroll
-            for (int r = 0; r < 8; ++r) {
-              const Real ox = __shfl_xor_sync(0xffffffffu, zx[r], 1), oy = __shfl_xor_sync(0xffffffffu, zy[r], 1);
-              zx[r] = half == 0 ? zx[r] + ox : ox - zx[r];
-              zy[r] = half == 0 ? zy[r] + oy : oy - zy[r];
-            }
-          } else {
-#pragma unroll
-            for (int r = 0; r < 8; ++r) {
-              zx[r] = remote(xs, r, phys<ES>(n));
-              zy[r] = remote(ys, r, phys<ES>(n));
-            }
-          }
-          whtr<Real, 8>(zx);
-          whtr<Real, 8>(zy);
-#pragma unroll
-          for (int jj = 0; jj < 8; ++jj) {
-            if constexpr (kF32) tsum(qh[u * 8 + jj][0], ql[u * 8 + jj][0], zx[jj] * zy[jj]);
-            else qd[u * 8 + jj][0] = fma(zx[jj], zy[jj], qd[u * 8 + jj][0]);
-          }
-        }
-      }
-      cluster.sync();  // reads of buffer (step - 1) & 1 retired
-      kk = kn;
-    }
-    {
-#pragma unroll
-      for (int o = 0; o < OUT; ++o) {
-        const int gi = gt + kWsGroup * (o >> 3);
-        const int64_t f = out_f(gi, o & 7);
-        double vx, vy;
-        if constexpr (kF32) {
-          vx = (double)qh[o][0] + (double)ql[o][0];
-          vy = (double)qh[o][QC - 1] + (double)ql[o][QC - 1];
-        } else {
-          vx = qd[o][0];
-          vy = qd[o][QC - 1];
-        }
-        if (kFFT) partC[f] = make_double2(vx, vy);
-        else partR[f] = vx;
-      }
-    }
-  }
-
-  }  // item loop
-}
-
 // ------------------------------------------------------------------ host
-// Which products run the warp-specialized kernels (L = 4096):
-// CMM_CLUSTER_WS = 0 none, 1 the plain path (FP64), all FP64 and FP32;
-// unset = 1.  The others run the single-group kernels (FP32 FFT: L = 8192;
-// FP32 FWHT: the tensor-core slab kernel).
-int cluster_ws_mode() {
-  static const int mode = [] {
-    const char* e = getenv("CMM_CLUSTER_WS");
-    if (e && !strcmp(e, "0")) return 0;
-    if (e && !strcmp(e, "all")) return 2;
-    return 1;
+// Where the staged rows come from: gathered from AT and B in place
+// (CMM_CLUSTER_ROWS=gather), or copied first, per chunk of inner indices, into
+// plan order with the sign applied (copy, the default).
+bool cluster_rows_gathered() {
+  static const bool g = [] {
+    const char* e = getenv("CMM_CLUSTER_ROWS");
+    return e && !strcmp(e, "gather");
   }();
-  return mode;
+  return g;
 }
 
-bool cluster_ws_for(bool f32) { return f32 ? cluster_ws_mode() == 2 : cluster_ws_mode() >= 1; }
-
-int cluster_log_slab(int variant, bool f32, bool ws) {
-  if (ws) return 12;
-  return (variant == kVariantFFT && !f32) ? 12 : 13;
-}
+int cluster_log_slab(int variant, bool f32) { return (variant == kVariantFFT && !f32) ? 12 : 13; }
 
 bool sketch_cluster_applicable(int variant, bool f32, int b) {
-  // mixed FWHT: the warp-specialized FP32 kernel when selected, else the
-  // tensor-core slab kernel
-  if (variant == kVariantFWHT && f32 && !cluster_ws_for(true)) return false;
+  if (variant == kVariantFWHT && f32) return false;  // mixed FWHT: tensor-core slab kernel
   int log2b = 0;
   while ((1 << log2b) < b) ++log2b;
-  // R = b / L >= 8 with the single-group slab lengths (FWHT: b >= 2^16); the
-  // DIF twiddle table covers b <= 2^19
-  return log2b - cluster_log_slab(variant, f32, false) >= 3 && log2b <= 19;
+  // R = b / L >= 8; the DIF twiddle table covers b <= 2^19
+  return log2b - cluster_log_slab(variant, f32) >= 3 && log2b <= 19;
 }
 
 constexpr size_t kClSmemMax = 227 * 1024;
@@ -1161,21 +726,11 @@ static void cl_kernel_attrs(size_t smem) {
   CMM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   CMM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
 }
-template <int V, typename Real>
-static void ws_kernel_attrs(size_t smem) {
-  auto k = k_sketch_cluster_ws<V, Real>;
-  CMM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  CMM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-}
 
 // shared bytes of one CTA and the buffer count: two sub-spectrum buffers
-// when they fit, else one (the warp-specialized kernels always use two)
-static size_t cl_smem(int variant, bool f32, bool ws, int R1, int log2b, int64_t SA, int64_t SB, int* nb) {
+// when they fit, else one
+static size_t cl_smem(int variant, bool f32, int R1, int log2b, int64_t SA, int64_t SB, int* nb) {
   const bool fft = variant == kVariantFFT;
-  if (ws) {
-    if (nb) *nb = 2;
-    return ws_layout(fft, f32, R1, log2b, SA, SB).total;
-  }
   const size_t two = cl_layout(fft, f32, 2, R1, log2b, SA, SB).total;
   if (two <= kClSmemMax) {
     if (nb) *nb = 2;
@@ -1213,21 +768,7 @@ static int max_clusters_of(K kernel, int threads, int R2, size_t smem) {
   return n;
 }
 
-static int cl_max_clusters(int variant, bool f32, bool ws, int R2, size_t smem) {
-  if (ws) {
-#define CMM_WS_MAX(V, T)                                                       \
-  do {                                                                         \
-    ws_kernel_attrs<V, T>(smem);                                               \
-    return max_clusters_of(k_sketch_cluster_ws<V, T>, 2 * kWsGroup, R2, smem); \
-  } while (0)
-    if (variant == kVariantFFT) {
-      if (f32) CMM_WS_MAX(0, float);
-      CMM_WS_MAX(0, double);
-    }
-    if (f32) CMM_WS_MAX(1, float);
-    CMM_WS_MAX(1, double);
-#undef CMM_WS_MAX
-  }
+static int cl_max_clusters(int variant, bool f32, int R2, size_t smem) {
   if (variant == kVariantFFT && f32) {
     cl_kernel_attrs<0, float, 1>(smem);
     return max_clusters_of(k_sketch_cluster<0, float, 1>, kCT, R2, smem);
@@ -1244,10 +785,9 @@ static int cl_max_clusters(int variant, bool f32, bool ws, int R2, size_t smem) 
 // co-resident clusters NC: the grid holds NC persistent clusters that share
 // the R1 * d * G work items round-robin; the estimate ceil(items/NC)/G is
 // minimised (ties to R2 = 16: less scatter redundancy, fewer items).
-ClusterPlan plan_cluster(int variant, bool f32, bool ws, int64_t n_inner, int d, int b, int64_t n_max) {
+ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, int64_t n_max) {
   ClusterPlan C;
-  C.ws = ws;
-  C.logL = cluster_log_slab(variant, f32, ws);
+  C.logL = cluster_log_slab(variant, f32);
   C.log2b = 0;
   while ((1 << C.log2b) < b) ++C.log2b;
   const int logR = C.log2b - C.logL;
@@ -1257,9 +797,9 @@ ClusterPlan plan_cluster(int variant, bool f32, bool ws, int64_t n_inner, int d,
     const int R2 = 1 << logR2, R1 = 1 << (logR - logR2);
     // expected largest residue segment: n / R2 plus a margin for the spread
     const int64_t est_slots = (n_max + R2 - 1) / R2 + (n_max + R2 - 1) / R2 / 8 + 64;
-    const size_t smem = cl_smem(variant, f32, ws, R1, C.log2b, est_slots, est_slots, nullptr);
+    const size_t smem = cl_smem(variant, f32, R1, C.log2b, est_slots, est_slots, nullptr);
     if (smem > kClSmemMax) continue;
-    const int mx = cl_max_clusters(variant, f32, ws, R2, smem);
+    const int mx = cl_max_clusters(variant, f32, R2, smem);
     if (mx <= 0) continue;
     const int64_t base = (int64_t)R1 * d;
     for (int64_t G = 1; G <= 64; ++G) {
@@ -1280,23 +820,25 @@ ClusterPlan plan_cluster(int variant, bool f32, bool ws, int64_t n_inner, int d,
   }
   if (best >= 1e299) throw unsupported("no cluster configuration fits this device");
   if (getenv("CMM_DEBUG"))
-    fprintf(stderr, "[cmm] cluster plan: b=%d L=%d R1=%d R2=%d G=%d clusters=%d ws=%d\n", b, 1 << C.logL,
-            1 << C.logR1, 1 << C.logR2, C.G, C.max_clusters, (int)ws);
+    fprintf(stderr, "[cmm] cluster plan: b=%d L=%d R1=%d R2=%d G=%d clusters=%d\n", b, 1 << C.logL,
+            1 << C.logR1, 1 << C.logR2, C.G, C.max_clusters);
   return C;
 }
 
 bool cluster_smem_fits(int variant, bool f32, const ClusterPlan& C, const SlabPlan& P) {
-  return cl_smem(variant, f32, C.ws, 1 << C.logR1, C.log2b, P.EA, P.EB, nullptr) <= kClSmemMax;
+  return cl_smem(variant, f32, 1 << C.logR1, C.log2b, P.EA, P.EB, nullptr) <= kClSmemMax;
 }
 
 void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const SlabPlan& P, const void* dA,
-                           const void* dB, int64_t kc, const int* dScaleExp, int64_t k0, const double2* dTw,
-                           void* dPartial, int d, int accumulate, cudaStream_t s) {
-  if (!P.owner || P.owner_logT != 9 || P.logL != C.logL)
-    throw runtime_error("cluster sketch: plan does not match the kernel");
+                           const void* dB, const void* dMatA, const void* dMatB, int64_t kc,
+                           const int* dScaleExp, int64_t k0, const double2* dTw, void* dPartial, int d,
+                           int accumulate, cudaStream_t s) {
+  if (!P.owner || P.logL != C.logL) throw runtime_error("cluster sketch: plan does not match the kernel");
   ClArgs a;
   a.A = dA;
   a.B = dB;
+  a.matA = dMatA;
+  a.matB = dMatB;
   a.lda = P.n_a;
   a.ldb = P.n_b;
   a.srcA = P.srcA.as<uint32_t>();
@@ -1320,33 +862,15 @@ void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const Sl
   a.accumulate = accumulate;
   const int R2 = 1 << C.logR2, R1 = 1 << C.logR1;
   int nb = 1;
-  const size_t smem = cl_smem(variant, f32, C.ws, R1, C.log2b, a.SA, a.SB, &nb);
+  const size_t smem = cl_smem(variant, f32, R1, C.log2b, a.SA, a.SB, &nb);
   if (smem > kClSmemMax) throw unsupported("cluster sketch: residue segments too large for shared memory");
   if (getenv("CMM_DEBUG"))
-    fprintf(stderr, "[cmm] cluster launch: smem=%zu buffers=%d SA=%lld SB=%lld ws=%d\n", smem, nb,
-            (long long)a.SA, (long long)a.SB, (int)C.ws);
+    fprintf(stderr, "[cmm] cluster launch: smem=%zu buffers=%d SA=%lld SB=%lld rows=%s\n", smem, nb,
+            (long long)a.SA, (long long)a.SB, dMatA ? "copied" : "gathered");
   const dim3 grid((unsigned)R2, (unsigned)C.max_clusters, 1);
   ProfScope prof("sketch", s);
   count_launch();
   cudaLaunchAttribute attr[1];
-  if (C.ws) {
-    const cudaLaunchConfig_t cfg = cluster_config(grid, 2 * kWsGroup, R2, smem, s, attr);
-#define CMM_WS(V, T)                                                   \
-  do {                                                                 \
-    ws_kernel_attrs<V, T>(smem);                                       \
-    CMM_CUDA(cudaLaunchKernelEx(&cfg, k_sketch_cluster_ws<V, T>, a));  \
-  } while (0)
-    if (variant == kVariantFFT) {
-      if (f32) CMM_WS(0, float);
-      else CMM_WS(0, double);
-    } else {
-      if (f32) CMM_WS(1, float);
-      else CMM_WS(1, double);
-    }
-#undef CMM_WS
-    CMM_CUDA(cudaGetLastError());
-    return;
-  }
   const cudaLaunchConfig_t cfg = cluster_config(grid, kCT, R2, smem, s, attr);
 #define CMM_CL(V, T)                                                   \
   do {                                                                 \

@@ -11,7 +11,8 @@ kernels (asserted through cmm_last_sketch_kernel) and cover:
   * all-zero rows, which every CTA of a cluster skips, including at the
     start and end of the inner range (the staged next row must follow);
   * chunked launches over streamed host rows (accumulating partials);
-  * rows gathered in place from AT and B (no per-repetition copies).
+  * the staged rows copied per chunk in slot order (the default) -- run the
+    file with CMM_CLUSTER_ROWS=gather for the in-place gathers.
 Tolerances: FP64 sketch within 1e-11 * max|p| absolute; mixed within
 2e-5 * max|p|.
 """
@@ -102,10 +103,10 @@ def test_chunked_launches_accumulate(gpu, oracle, variant, b):
     check(variant, None, AT, B, 3, b, 21, oracle)
 
 
-def test_gather_reads_rows_in_place(gpu, oracle):
-    """The kernels gather each row's segment from AT and B directly, with
-    the sign applied per slot: rows of very different scales in A and B
-    (the FFT row balance) and a planted large entry, both variants."""
+def test_unbalanced_rows_and_signs(gpu, oracle):
+    """Each slot's sign is applied once (by the row copy, or per slot when
+    gathering): rows of very different scales in A and B (the FFT row
+    balance) and a planted large entry, both variants."""
     rng = np.random.default_rng(19)
     AT = rng.standard_normal((50, 333)) * np.logspace(-3, 3, 50)[:, None]
     B = rng.standard_normal((50, 277)) * np.logspace(3, -3, 50)[:, None]
