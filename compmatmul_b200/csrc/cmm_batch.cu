@@ -41,7 +41,6 @@ constexpr int kBT = 1024;        // threads per CTA
 constexpr int kBFftLog = kBatchFftLog;
 constexpr int kBWhtLog = kBatchWhtLog;
 constexpr int kBSkip = -0x7fffffff;
-constexpr int kBatchSlots = 4;   // slots whose loads the scatter issues together
 
 using namespace dev;
 
@@ -341,26 +340,10 @@ __global__ void __launch_bounds__(kBT, 1)
                                  : (Real)__longlong_as_double((long long)(1023 + e2) << 52);
             C* arr = side ? bufB(q) : bufA(q);
             C run = mk((Real)0, (Real)0);
-            for (int sl0 = beg; sl0 < end; sl0 += kBatchSlots) {
-              // the indices and codes of a few slots, then their row values:
-              // the dependent loads of several slots are in flight together
-              uint32_t svs[kBatchSlots], hs[kBatchSlots];
-              Real vs[kBatchSlots];
-#pragma unroll
-              for (int u = 0; u < kBatchSlots; ++u) {
-                const bool ok = sl0 + u < end;
-                svs[u] = ok ? __ldg(src + sl0 + u) : 0u;
-                hs[u] = ok ? (P.code16 ? (uint32_t)__ldg(c16 + sl0 + u) : __ldg(c32 + sl0 + u)) : 0u;
-              }
-#pragma unroll
-              for (int u = 0; u < kBatchSlots; ++u)
-                vs[u] = sl0 + u < end ? __ldg(row + (svs[u] & 0x7fffffffu)) : (Real)0;
-#pragma unroll
-              for (int u = 0; u < kBatchSlots; ++u) {
-              if (sl0 + u >= end) break;
-              const uint32_t sv = svs[u];
-              const uint32_t h = hs[u];
-              Real v = vs[u] * sc;
+            for (int sl = beg; sl < end; ++sl) {
+              const uint32_t sv = __ldg(src + sl);
+              const uint32_t h = P.code16 ? (uint32_t)__ldg(c16 + sl) : __ldg(c32 + sl);
+              Real v = __ldg(row + (sv & 0x7fffffffu)) * sc;
               if (!(sv >> 31)) v = -v;
               C c;
               if (r == 0) {
@@ -381,30 +364,15 @@ __global__ void __launch_bounds__(kBT, 1)
               } else {
                 run = mk(run.x + c.x, run.y + c.y);
               }
-              }
             }
             if (cur != 0xffffffffu) arr[ph<EC>(brev_bits(cur, logL))] = run;
           } else {
             Real* arr = side ? ysq(q) : xsq(q);
             Real run = (Real)0;
-            for (int sl0 = beg; sl0 < end; sl0 += kBatchSlots) {
-              uint32_t svs[kBatchSlots], hs[kBatchSlots];
-              Real vs[kBatchSlots];
-#pragma unroll
-              for (int u = 0; u < kBatchSlots; ++u) {
-                const bool ok = sl0 + u < end;
-                svs[u] = ok ? __ldg(src + sl0 + u) : 0u;
-                hs[u] = ok ? (P.code16 ? (uint32_t)__ldg(c16 + sl0 + u) : __ldg(c32 + sl0 + u)) : 0u;
-              }
-#pragma unroll
-              for (int u = 0; u < kBatchSlots; ++u)
-                vs[u] = sl0 + u < end ? __ldg(row + (svs[u] & 0x7fffffffu)) : (Real)0;
-#pragma unroll
-              for (int u = 0; u < kBatchSlots; ++u) {
-              if (sl0 + u >= end) break;
-              const uint32_t sv = svs[u];
-              const uint32_t h = hs[u];
-              Real v = vs[u];
+            for (int sl = beg; sl < end; ++sl) {
+              const uint32_t sv = __ldg(src + sl);
+              const uint32_t h = P.code16 ? (uint32_t)__ldg(c16 + sl) : __ldg(c32 + sl);
+              Real v = __ldg(row + (sv & 0x7fffffffu));
               // sign(+-1) * (-1)^{popc(q & r)}: negate when the parity bit differs
               if (((sv >> 31) ^ 1u) ^ (__popc((h >> logL) & r) & 1u)) v = -v;
               const uint32_t m = h & (uint32_t)(L - 1);
@@ -414,7 +382,6 @@ __global__ void __launch_bounds__(kBT, 1)
                 run = v;
               } else {
                 run += v;
-              }
               }
             }
             if (cur != 0xffffffffu) arr[ph<ER>((int)cur)] = run;

@@ -306,29 +306,13 @@ static bool try_cluster_plan(int variant, bool f32, const Codes& codes, int64_t 
   // (513 against 545 ms of sketch kernel at b = 2^18)
   if (sketch_kernel_choice() == 0 && variant == kVariantFWHT && f32) return false;
   try {
-    C = plan_cluster(variant, f32, n_inner, sp.d, sp.b, n_a > n_b ? n_a : n_b);
+    C = plan_cluster(variant, f32, n_inner, sp.d, sp.b, 4096);
   } catch (const unsupported&) {
     return false;
   }
-  plan = make_owner_plan(codes.a.as<uint32_t>(), codes.b.as<uint32_t>(), n_a, n_b, sp.d, sp.b, C.logL, C.logR2,
-                         variant, s);
+  plan = make_residue_plan(codes.a.as<uint32_t>(), codes.b.as<uint32_t>(), n_a, n_b, sp.d, sp.b,
+                           C.logL, C.logR2, s);
   return cluster_smem_fits(variant, f32, C, plan);
-}
-
-// Inner indices per cluster-kernel launch.  Copied rows: as many as the
-// copy budget holds (the first chunk an eighth of that while rows still
-// arrive from the host).  Gathered rows: all of them for device inputs,
-// an eighth (at least 64) for host inputs, so each launch overlaps the
-// copies of the next piece.
-static int64_t cluster_chunk(int64_t n_inner, int64_t per_row_bytes, const RowFeed* feed) {
-  if (!cluster_rows_gathered()) {
-    int64_t kc = (int64_t)(materialize_budget() / (size_t)per_row_bytes);
-    if (kc < 1) kc = 1;
-    return kc < n_inner ? kc : n_inner;
-  }
-  if (!feed) return n_inner;
-  const int64_t c = n_inner / 8;
-  return c < 64 ? (n_inner < 64 ? n_inner : 64) : c;
 }
 
 // Inner indices of the sketch chunk starting at k0.  While rows are still
@@ -357,22 +341,20 @@ static void sketch_device(int variant, const SketchParams& sp, const Codes& code
   ClusterPlan C;
   SlabPlan plan;
   if (n_inner > 0 && try_cluster_plan(variant, false, codes, n_a, n_b, n_inner, sp, C, plan, s)) {
-    // owner plan + cluster kernels; rows copied per chunk in slot order (or gathered)
+    // residue plan + per-chunk materialized rows + cluster kernels
     set_sketch_kernel("cluster");
-    const bool gathered = cluster_rows_gathered();
     const int64_t SA = plan.slots_a(), SB = plan.slots_b();
-    const int64_t kc = cluster_chunk(n_inner, (int64_t)sp.d * (SA + SB) * 8, feed);
-    DevBuf matA, matB;
-    if (!gathered) {
-      matA = DevBuf((size_t)sp.d * kc * SA * 8, s);
-      matB = DevBuf((size_t)sp.d * kc * SB * 8, s);
-    }
+    const size_t per_row = (size_t)sp.d * (size_t)(SA + SB) * 8;
+    int64_t kc = (int64_t)(materialize_budget() / per_row);
+    if (kc < 1) kc = 1;
+    if (kc > n_inner) kc = n_inner;
+    DevBuf matA((size_t)sp.d * kc * SA * 8, s), matB((size_t)sp.d * kc * SB * 8, s);
     DevBuf partial((size_t)C.G * sp.d * (size_t)sp.b * elem, s);
     for (int64_t k0 = 0, c = 0; k0 < n_inner; k0 += c) {
       c = chunk_len(k0, kc, n_inner, feed);
       rows_ready(k0, c);
-      if (!gathered) launch_materialize(plan, dAT, dB, k0, c, matA.as<double>(), matB.as<double>(), s);
-      launch_sketch_cluster(variant, false, C, plan, dAT, dB, matA.ptr, matB.ptr, c, scale.as<int>(), k0, tw,
+      launch_materialize(plan, dAT, dB, k0, c, matA.as<double>(), matB.as<double>(), s);
+      launch_sketch_cluster(variant, false, C, plan, matA.ptr, matB.ptr, c, scale.as<int>(), k0, tw,
                             partial.ptr, sp.d, k0 > 0 ? 1 : 0, s);
     }
     DevBuf work(2 * (size_t)sp.d * (size_t)sp.b * 16, s);
@@ -440,20 +422,19 @@ static void sketch_device_mixed(int variant, const SketchParams& sp, const Codes
   SlabPlan cplan;
   if (try_cluster_plan(variant, true, codes, n_a, n_b, n_inner, sp, Cp, cplan, s)) {
     set_sketch_kernel("cluster");
-    const bool gathered = cluster_rows_gathered();
-    const int64_t SA = cplan.slots_a(), SB = cplan.slots_b();
-    const int64_t kc = cluster_chunk(n_inner, (int64_t)sp.d * (SA + SB) * 4, feed);
-    DevBuf matA, matB;
-    if (!gathered) {
-      matA = DevBuf((size_t)sp.d * kc * SA * 4, s);
-      matB = DevBuf((size_t)sp.d * kc * SB * 4, s);
-    }
+    SlabPlan& plan = cplan;
+    const int64_t SA = plan.slots_a(), SB = plan.slots_b();
+    const size_t per_row = (size_t)sp.d * (size_t)(SA + SB) * 4;
+    int64_t kc = (int64_t)(materialize_budget() / per_row);
+    if (kc < 1) kc = 1;
+    if (kc > n_inner) kc = n_inner;
+    DevBuf matA((size_t)sp.d * kc * SA * 4, s), matB((size_t)sp.d * kc * SB * 4, s);
     DevBuf partial((size_t)Cp.G * sp.d * (size_t)sp.b * elem, s);
     for (int64_t k0 = 0, c = 0; k0 < n_inner; k0 += c) {
       c = chunk_len(k0, kc, n_inner, feed);
       rows_ready(k0, c);
-      if (!gathered) launch_materialize_f32(cplan, dAT, dB, k0, c, matA.as<float>(), matB.as<float>(), s);
-      launch_sketch_cluster(variant, true, Cp, cplan, dAT, dB, matA.ptr, matB.ptr, c, scale.as<int>(), k0, tw,
+      launch_materialize_f32(plan, dAT, dB, k0, c, matA.as<float>(), matB.as<float>(), s);
+      launch_sketch_cluster(variant, true, Cp, plan, matA.ptr, matB.ptr, c, scale.as<int>(), k0, tw,
                             partial.ptr, sp.d, k0 > 0 ? 1 : 0, s);
     }
     DevBuf work(2 * (size_t)sp.d * (size_t)sp.b * 16, s);

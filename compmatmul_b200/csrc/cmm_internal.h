@@ -169,7 +169,6 @@ struct SlabPlan {
   int64_t slots_a() const { return (int64_t)segs * EA * (compact ? 1 : kPlanThreads); }
   int64_t slots_b() const { return (int64_t)segs * EB * (compact ? 1 : kPlanThreads); }
   bool u16 = true;  // codes stored as u16 (b <= 2^16)
-  bool owner = false;  // owner plan (cluster kernels): slots by first-pass owner thread
   int64_t n_a = 0, n_b = 0;
   DevBuf srcA, srcB;      // d x S: index | (sign == +1) << 31, or kPadSlot
   DevBuf codeA, codeB;    // d x S: bucket h
@@ -177,12 +176,7 @@ struct SlabPlan {
 };
 SlabPlan make_slab_plan(const uint32_t* dCodesA, const uint32_t* dCodesB, int64_t n_a, int64_t n_b,
                         int d, int b, int logL, cudaStream_t s);
-// owner plans for the cluster kernels (b = R1 * R2 * L): slots of each
-// residue segment sorted by the thread whose first radix pass reads their
-// sub-bucket; src = index, code = q | q1 << 4 | (sign == +1) << 15
-SlabPlan make_owner_plan(const uint32_t* dCodesA, const uint32_t* dCodesB, int64_t n_a, int64_t n_b, int d,
-                         int b, int logL, int logR2, int variant, cudaStream_t s);
-// residue plans (b = R1 * R2 * L)
+// residue plans for the cluster kernels (b = R1 * R2 * L)
 SlabPlan make_residue_plan(const uint32_t* dCodesA, const uint32_t* dCodesB, int64_t n_a, int64_t n_b,
                            int d, int b, int logL, int logR2, cudaStream_t s);
 void launch_materialize(const SlabPlan& P, const double* dAT, const double* dB, int64_t k0,
@@ -212,23 +206,17 @@ void launch_materialize_f32(const SlabPlan& P, const float* dAT, const float* dB
 void launch_f32_to_f64(const float* src, double* dst, int64_t n, cudaStream_t s);
 
 // Cluster kernels (cmm_sketch_cluster.cu): b = R1 * R2 * L; partials in
-// natural frequency order [g][t][b], over an owner plan (make_owner_plan).
+// natural frequency order [g][t][b].
 struct ClusterPlan {
   int logL = 0, log2b = 0, logR1 = 0, logR2 = 0, G = 1, max_clusters = 0;
 };
-bool cluster_rows_gathered();  // CMM_CLUSTER_ROWS=gather: no row copies
-int cluster_log_slab(int variant, bool f32);
 bool sketch_cluster_applicable(int variant, bool f32, int b);
-// n_max = max(n_a, n_b): sizes the residue segments for the shared-memory estimate
-ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, int64_t n_max);
+ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, int64_t est_slots);
 bool cluster_smem_fits(int variant, bool f32, const ClusterPlan& C, const SlabPlan& P);
-// inner indices [k0, k0 + kc) of dA / dB (FP64, or FP32 when f32); dMatA /
-// dMatB: the chunk's rows copied in slot order (launch_materialize), or
-// NULL to gather from dA / dB
-void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const SlabPlan& P, const void* dA,
-                           const void* dB, const void* dMatA, const void* dMatB, int64_t kc,
-                           const int* dScaleExp, int64_t k0, const double2* dTw, void* dPartial, int d,
-                           int accumulate, cudaStream_t s);
+void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const SlabPlan& P,
+                           const void* dMatA, const void* dMatB, int64_t kc, const int* dScaleExp,
+                           int64_t k0, const double2* dTw, void* dPartial, int d, int accumulate,
+                           cudaStream_t s);
 // finalize for partials in natural frequency order (cluster kernels)
 void launch_finalize_natural(int variant, int d, int b, int G, const void* dPartial,
                              const double2* dTw, void* dWork, double* dP, cudaStream_t s);

@@ -468,203 +468,3 @@ SlabPlan make_residue_plan(const uint32_t* dCodesA, const uint32_t* dCodesB, int
 }
 
 }  // namespace cmm
-
-namespace cmm {
-
-// ------------------------------------------------------- owner plans
-// Plans for the cluster kernels (cmm_sketch_cluster.cu), which read the
-// input rows directly (no materialized copies) and fuse the count sketch
-// into their first radix pass.  With b = R1 * R2 * L, an index with bucket
-// h belongs to residue class r2 = h mod R2, sub-bucket m = (h mod (b / R1))
-// div R2 (< L) and DIF quotient q1 = h div (b / R1), as for residue plans.
-// The first pass of the CTA's L-point transform is done by T = 2^logT = 512
-// threads, thread j on the QN = L / T points j * QN + e; so thread j owns
-// the sub-buckets those points hold:
-//   FFT  (bit-reversed input): m = brev(j * QN + e) -> j = brev_logT(m mod T),
-//        element q = m div T (e = brev(q));
-//   FWHT (natural order):      m = j * QN + e       -> j = m div QN, q = m mod QN.
-// Per (t, side, r2) the members are stably sorted by (owner j, q); thread
-// j's slots are [cut[j], cut[j + 1]).  A slot holds src = index |
-// (sign == +1) << 31 (kPadSlot past the segment's end, as the residue plans,
-// so k_materialize can copy the rows in slot order) and the code
-// q | q1 << 4 | (sign == +1) << 15.
-// logT = log2 of the threads sharing the first pass
-__device__ __forceinline__ uint32_t owner_key(uint32_t m, int logL, int logT, bool fft) {
-  if (!fft) return m;
-  const uint32_t tmask = (1u << logT) - 1u;
-  return ((__brev(m & tmask) >> (32 - logT)) << (logL - logT)) | (m >> logT);
-}
-
-__global__ void __launch_bounds__(kSegSortThreads) k_plan_owner_sort(
-    const uint32_t* __restrict__ codesA, const uint32_t* __restrict__ codesB, int64_t n_a, int64_t n_b,
-    int logL, int logR2, int logM, int logT, int fft, uint32_t* __restrict__ sortedA,
-    uint32_t* __restrict__ sortedB, uint32_t* __restrict__ cut, uint32_t* __restrict__ emax) {
-  extern __shared__ uint32_t sown[];
-  const int L = 1 << logL, R2 = 1 << logR2;
-  uint32_t* cnt = sown;
-  uint32_t* cum = sown + L + 1;
-  const int t = blockIdx.x, side = blockIdx.y, r2 = blockIdx.z;
-  const int64_t N = side == 0 ? n_a : n_b;
-  const uint32_t* codes = (side == 0 ? codesA : codesB) + (size_t)t * N;
-  uint32_t* sorted = (side == 0 ? sortedA : sortedB) + ((size_t)t * R2 + r2) * N;
-  const uint32_t rmask = (uint32_t)R2 - 1u, mmask = (1u << logM) - 1u;
-  for (int e = threadIdx.x; e <= L; e += kSegSortThreads) cnt[e] = 0;
-  __syncthreads();
-  for (int64_t i = threadIdx.x; i < N; i += kSegSortThreads) {
-    const uint32_t h = __ldg(codes + i) & 0x7fffffffu;
-    if ((h & rmask) == (uint32_t)r2) atomicAdd(&cnt[owner_key((h & mmask) >> logR2, logL, logT, fft)], 1u);
-  }
-  __syncthreads();
-  if (threadIdx.x < 32) {  // exclusive scan of cnt[0..L) into cum
-    const int lane = threadIdx.x;
-    const int per = (L + 31) / 32;
-    uint32_t local = 0;
-    for (int e = lane * per; e < (lane + 1) * per && e < L; ++e) local += cnt[e];
-    uint32_t incl = local;
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += v;
-    }
-    uint32_t run = incl - local;
-    for (int e = lane * per; e < (lane + 1) * per && e < L; ++e) {
-      const uint32_t c = cnt[e];
-      cum[e] = run;
-      run += c;
-    }
-    if (lane == 31) cum[L] = incl;
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e <= L; e += kSegSortThreads) cnt[e] = cum[e];
-  __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int64_t base = 0; base < N; base += kSegSortThreads) {  // stable placement
-    const int64_t i = base + threadIdx.x;
-    bool valid = i < N;
-    uint32_t key = 0x80000000u | (uint32_t)lane;
-    if (valid) {
-      const uint32_t h = __ldg(codes + i) & 0x7fffffffu;
-      valid = (h & rmask) == (uint32_t)r2;
-      if (valid) key = owner_key((h & mmask) >> logR2, logL, logT, fft);
-    }
-    const uint32_t peers = __match_any_sync(0xffffffffu, key);
-    const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
-    for (int w = 0; w < kSegSortThreads / 32; ++w) {
-      if (warp == w && valid) sorted[cnt[key] + rank] = (uint32_t)i;
-      __syncwarp();
-      if (warp == w && valid && rank == 0) cnt[key] += __popc(peers);
-      __syncthreads();
-    }
-  }
-  // thread j of the sketch kernel owns keys [j * QN, (j + 1) * QN)
-  const int QB = logL - logT;
-  uint32_t* cuts = cut + (((size_t)t * 2 + side) * R2 + r2) * (kPlanThreads + 1);
-  for (int j = threadIdx.x; j <= kPlanThreads; j += kSegSortThreads)
-    cuts[j] = j <= (1 << logT) ? cum[j << QB] : cum[L];
-  if (threadIdx.x == 0) emax[((size_t)t * 2 + side) * R2 + r2] = cum[L];  // segment size
-}
-
-__global__ void k_plan_owner_layout(const uint32_t* __restrict__ codesA, const uint32_t* __restrict__ codesB,
-                                    int64_t n_a, int64_t n_b, int logL, int logR2, int logM, int logT, int fft,
-                                    int R2, const uint32_t* __restrict__ sortedA,
-                                    const uint32_t* __restrict__ sortedB,
-                                    const uint32_t* __restrict__ cut, int SA, int SB, uint32_t* __restrict__ srcA,
-                                    uint32_t* __restrict__ srcB, uint16_t* __restrict__ codeA,
-                                    uint16_t* __restrict__ codeB, uint32_t* __restrict__ cutA,
-                                    uint32_t* __restrict__ cutB) {
-  const int t = blockIdx.y;
-  const int side = blockIdx.z & 1, r2 = blockIdx.z >> 1;
-  const int S = side == 0 ? SA : SB;
-  const int64_t N = side == 0 ? n_a : n_b;
-  const uint32_t* codes = (side == 0 ? codesA : codesB) + (size_t)t * N;
-  const uint32_t* sorted = (side == 0 ? sortedA : sortedB) + ((size_t)t * R2 + r2) * N;
-  const uint32_t* cuts = cut + (((size_t)t * 2 + side) * R2 + r2) * (kPlanThreads + 1);
-  const uint32_t total = cuts[kPlanThreads];
-  uint32_t* src = (side == 0 ? srcA : srcB) + ((size_t)t * R2 + r2) * S;
-  uint16_t* code = (side == 0 ? codeA : codeB) + ((size_t)t * R2 + r2) * S;
-  const uint32_t mmask = (1u << logM) - 1u, qmask = (1u << (logL - logT)) - 1u;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < S; e += (int64_t)gridDim.x * blockDim.x) {
-    if ((uint32_t)e < total) {
-      const uint32_t i = sorted[e];
-      const uint32_t c = codes[i];
-      const uint32_t h = c & 0x7fffffffu;
-      const uint32_t q = owner_key((h & mmask) >> logR2, logL, logT, fft) & qmask;
-      src[e] = i | (c & 0x80000000u);
-      code[e] = (uint16_t)(q | ((h >> logM) << 4) | ((c >> 31) << 15));
-    } else {
-      src[e] = kPadSlot;
-      code[e] = 0;
-    }
-  }
-  if (blockIdx.x == 0)
-    for (int j = threadIdx.x; j <= kPlanThreads; j += blockDim.x)
-      (side == 0 ? cutA : cutB)[((size_t)t * R2 + r2) * (kPlanThreads + 1) + j] = cuts[j];
-}
-
-SlabPlan make_owner_plan(const uint32_t* dCodesA, const uint32_t* dCodesB, int64_t n_a, int64_t n_b, int d,
-                         int b, int logL, int logR2, int variant, cudaStream_t s) {
-  const int logT = 9;  // the cluster kernels' kPlanThreads first-pass threads
-  SlabPlan P;
-  P.d = d;
-  P.logL = logL;
-  P.n_a = n_a;
-  P.n_b = n_b;
-  int log2b = 0;
-  while ((1 << log2b) < b) ++log2b;
-  const int logR1 = log2b - logL - logR2;
-  const int logM = log2b - logR1;
-  if (logL < logT || logL - logT > 4 || logR1 > 11)
-    throw unsupported("owner plan: slab length or DIF radix out of range");
-  P.segs = 1 << logR2;
-  P.u16 = true;
-  P.owner = true;
-  const int L = 1 << logL, R2 = 1 << logR2;
-  const int fft = variant == kVariantFFT ? 1 : 0;
-  DevBuf sortedA((size_t)d * R2 * (n_a > 0 ? n_a : 1) * 4, s), sortedB((size_t)d * R2 * (n_b > 0 ? n_b : 1) * 4, s);
-  DevBuf cut((size_t)d * 2 * R2 * (kPlanThreads + 1) * 4, s), emax((size_t)d * 2 * R2 * 4, s);
-  const int smem = 2 * (L + 1) * 4;
-  CMM_CUDA(cudaFuncSetAttribute(k_plan_owner_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  {
-    ProfScope prof("plan", s);
-    count_launch();
-    k_plan_owner_sort<<<dim3(d, 2, R2), kSegSortThreads, smem, s>>>(
-        dCodesA, dCodesB, n_a, n_b, logL, logR2, logM, logT, fft, sortedA.as<uint32_t>(),
-        sortedB.as<uint32_t>(), cut.as<uint32_t>(), emax.as<uint32_t>());
-    CMM_CUDA(cudaGetLastError());
-  }
-  // segments hold S slots: the largest segment over (t, r2), rounded to 8
-  uint32_t SA = 8, SB = 8;
-  {
-    std::vector<uint32_t> h((size_t)d * 2 * R2);
-    CMM_CUDA(cudaMemcpyAsync(h.data(), emax.ptr, h.size() * 4, cudaMemcpyDeviceToHost, s));
-    CMM_CUDA(cudaStreamSynchronize(s));
-    for (int t = 0; t < d; ++t)
-      for (int r = 0; r < R2; ++r) {
-        SA = h[((size_t)t * 2 + 0) * R2 + r] > SA ? h[((size_t)t * 2 + 0) * R2 + r] : SA;
-        SB = h[((size_t)t * 2 + 1) * R2 + r] > SB ? h[((size_t)t * 2 + 1) * R2 + r] : SB;
-      }
-  }
-  SA = (SA + 7) & ~7u;
-  SB = (SB + 7) & ~7u;
-  P.compact = true;
-  P.EA = (int)SA;
-  P.EB = (int)SB;
-  P.srcA = DevBuf((size_t)d * R2 * SA * 4, s);
-  P.srcB = DevBuf((size_t)d * R2 * SB * 4, s);
-  P.codeA = DevBuf((size_t)d * R2 * SA * 2, s);
-  P.codeB = DevBuf((size_t)d * R2 * SB * 2, s);
-  P.countA = DevBuf((size_t)d * R2 * (kPlanThreads + 1) * 4, s);
-  P.countB = DevBuf((size_t)d * R2 * (kPlanThreads + 1) * 4, s);
-  const size_t Smax = SA > SB ? SA : SB;
-  dim3 grid((unsigned)((Smax + 255) / 256 < 256 ? (Smax + 255) / 256 : 256), (unsigned)d, (unsigned)(2 * R2));
-  ProfScope prof("plan", s);
-  count_launch();
-  k_plan_owner_layout<<<grid, 256, 0, s>>>(dCodesA, dCodesB, n_a, n_b, logL, logR2, logM, logT, fft, R2,
-                                           sortedA.as<uint32_t>(), sortedB.as<uint32_t>(), cut.as<uint32_t>(),
-                                           (int)SA, (int)SB, P.srcA.as<uint32_t>(), P.srcB.as<uint32_t>(),
-                                           P.codeA.as<uint16_t>(), P.codeB.as<uint16_t>(),
-                                           P.countA.as<uint32_t>(), P.countB.as<uint32_t>());
-  CMM_CUDA(cudaGetLastError());
-  return P;
-}
-
-}  // namespace cmm

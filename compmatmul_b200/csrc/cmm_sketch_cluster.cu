@@ -14,35 +14,22 @@
 //    cluster, reading the other CTAs' shared memory (DSMEM): CTA r2 owns the
 //    frequencies of L / R2 sub-spectrum positions and accumulates
 //    Z^2 (FFT, z = alpha x + i beta y) or X * Y (FWHT) for them over k.
-//
-// Rows reach the staging area in one of two ways, both in the plan's slot
-// order, one row ahead of the one being transformed: copied contiguously
-// from per-chunk copies of the rows (k_materialize writes each repetition's
-// segments with the sign applied), or gathered from the rows of AT and B
-// in place with cp.async, one 8-byte (or 4-byte) load per slot.  The copy
-// is the default: on B200 the gathers of a config-2 product (about 10^10
-// scattered 8-byte loads) cost more than writing and re-reading the copies.
-//
-// The count sketch is fused into the first radix pass: the owner plan
-// (cmm_plan.cu) sorts a segment by the thread whose first butterfly reads
-// each sub-bucket, so a thread sums its slots straight into the registers of
-// that butterfly (no zeroing, no shared-memory scatter, no barrier between
-// the sketch and the transform).
-//
-// With two sub-spectrum buffers (when they fit in shared memory) one
-// cluster barrier per inner index both publishes the new sub-spectra and
-// retires the reads of the buffer written next; with one buffer a second
-// barrier follows the combine.  Every CTA of a cluster runs the same k
-// sequence (all-zero rows are skipped by all of them), so all of them reach
-// every barrier.
-// Instantiations: FFT x FP64/FP32 (FP32 = mixed precision: FP32 data,
-// two-sum compensated accumulation, FP64 partials), FWHT x FP64; one or two
-// buffers.
+//  With two sub-spectrum buffers (when they fit in shared memory) one
+//  cluster barrier per inner index both publishes the new sub-spectra and
+//  retires the reads of the buffer written next; with one buffer a second
+//  barrier follows the combine.  Every CTA of a cluster runs the same k
+//  sequence (all-zero rows are skipped by all of them), so all of them
+//  reach every barrier.
+//  The next row's segments are staged with cp.async while the current one
+//  is transformed and combined.
+// Instantiations: FFT/FWHT x FP64/FP32 (FP32 = mixed precision: FP32 data,
+// two-sum compensated accumulation, tensor-core Hadamard-16 stages for the
+// FWHT, FP64 partials) x one or two buffers.
 #include <cooperative_groups.h>
+#include <cuda_bf16.h>
 
 #include <cstdio>
 #include <cstdlib>
-#include <cstring>
 
 #include "cmm_fft_device.cuh"
 #include "cmm_internal.h"
@@ -53,6 +40,7 @@ namespace cmm {
 namespace {
 
 constexpr int kCT = kPlanThreads;  // 512
+constexpr int kCBatch = 4;  // scatter slots loaded together
 constexpr int kCSkip = -0x7fffffff;
 
 using namespace dev;
@@ -68,7 +56,9 @@ __device__ __forceinline__ void dft8(C (&u)[8]) {
 }
 
 // padded shared layouts: 16- and 8-byte elements p + p/16, 4-byte p + p/32.
-// One spare element per 16 keeps the radix passes conflict-free.
+// One spare element per 16 keeps the radix passes conflict-free and spreads
+// the scatter's bit-reversed positions (a warp's buckets differ in bits that
+// land in p/16) over all banks.
 template <int ES>
 __device__ __forceinline__ int phys(int p) {
   return ES == 4 ? p + (p >> 5) : p + (p >> 4);
@@ -78,68 +68,74 @@ constexpr int phys_len(int L) {
   return ES == 4 ? L + L / 32 : L + L / 16;
 }
 
-// bit reversal of the B low bits (compile-time for unrolled loop indices)
-template <int B>
-__host__ __device__ constexpr int brev_bits(int x) {
-  int r = 0;
-  for (int i = 0; i < B; ++i) r |= ((x >> i) & 1) << (B - 1 - i);
-  return r;
+// ------------------------------------------------- tensor-core H16 (FP32)
+__device__ __forceinline__ uint32_t bf16x2(float lo_e, float hi_e) {
+  return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(lo_e)) |
+         ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(hi_e)) << 16);
 }
-
-// Element idx of the same shared array in the CTA of cluster rank `rank`:
-// a 32-bit shared::cluster address from mapa, read with ld.shared::cluster.
-// The loads are volatile, so they stay after the cluster barrier that
-// publishes the data (the barrier is a volatile asm too).
-__device__ __forceinline__ uint32_t cluster_addr(const void* local, int rank) {
-  uint32_t r;
-  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n"
-               : "=r"(r)
-               : "r"((uint32_t)__cvta_generic_to_shared(local)), "r"(rank));
-  return r;
+__device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_t& lo) {
+  const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
+  hi = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+  lo = bf16x2(x0 - __bfloat162float(h0), x1 - __bfloat162float(h1));
 }
-__device__ __forceinline__ void ld_cluster(double2& v, uint32_t a) {
-  asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];\n" : "=d"(v.x), "=d"(v.y) : "r"(a));
+__device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
-__device__ __forceinline__ void ld_cluster(float2& v, uint32_t a) {
-  asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];\n" : "=f"(v.x), "=f"(v.y) : "r"(a));
+template <int STAGE>
+__device__ __forceinline__ int hpt(int V, int e) {
+  if (STAGE == 0) return V * 16 + e;
+  if (STAGE == 1) return (V >> 4) * 256 + e * 16 + (V & 15);
+  return (V >> 8) * 4096 + e * 256 + (V & 255);
 }
-__device__ __forceinline__ void ld_cluster(double& v, uint32_t a) {
-  asm volatile("ld.shared::cluster.f64 %0, [%1];\n" : "=d"(v) : "r"(a));
-}
-__device__ __forceinline__ void ld_cluster(float& v, uint32_t a) {
-  asm volatile("ld.shared::cluster.f32 %0, [%1];\n" : "=f"(v) : "r"(a));
-}
-template <typename T>
-__device__ __forceinline__ T remote(const T* local_array, int rank, int idx) {
-  T v;
-  ld_cluster(v, cluster_addr(local_array + idx, rank));
-  return v;
+template <int STAGE>
+__device__ __forceinline__ void h16(float* buf, const uint32_t (&hb)[2][2], int warp, int lane) {
+  const int gq = lane >> 2, tq = lane & 3;
+  for (int tile = warp; tile < 32; tile += kCT / 32) {
+    const int V0 = tile * 16;
+    const int p[8] = {hpt<STAGE>(V0 + gq, 2 * tq),     hpt<STAGE>(V0 + gq, 2 * tq + 1),
+                      hpt<STAGE>(V0 + gq + 8, 2 * tq), hpt<STAGE>(V0 + gq + 8, 2 * tq + 1),
+                      hpt<STAGE>(V0 + gq, 2 * tq + 8), hpt<STAGE>(V0 + gq, 2 * tq + 9),
+                      hpt<STAGE>(V0 + gq + 8, 2 * tq + 8), hpt<STAGE>(V0 + gq + 8, 2 * tq + 9)};
+    float x[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) x[e] = buf[phys<4>(p[e])];
+    uint32_t ahi[4], alo[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) split2(x[2 * e], x[2 * e + 1], ahi[e], alo[e]);
+    float c0[4] = {0.f, 0.f, 0.f, 0.f}, c1[4] = {0.f, 0.f, 0.f, 0.f};
+    mma16816(c0, ahi, hb[0][0], hb[0][1]);
+    mma16816(c0, alo, hb[0][0], hb[0][1]);
+    mma16816(c1, ahi, hb[1][0], hb[1][1]);
+    mma16816(c1, alo, hb[1][0], hb[1][1]);
+    const float y[8] = {c0[0], c0[1], c0[2], c0[3], c1[0], c1[1], c1[2], c1[3]};
+#pragma unroll
+    for (int e = 0; e < 8; ++e) buf[phys<4>(p[e])] = y[e];
+  }
 }
 
 }  // namespace
 
 struct ClArgs {
-  const void* A;          // AT (n_inner x lda), row k at A + k * lda
-  const void* B;          // B (n_inner x ldb)
-  const void* matA;       // or NULL: rows k0 .. k0 + kc copied in slot order, sign applied,
-  const void* matB;       //   [t][kk][R2][SA] (then A / B are not read)
-  int64_t lda, ldb;
-  const uint32_t* srcA;   // [t][R2][SA] index | (sign == +1) << 31 of each slot
-  const uint32_t* srcB;
-  const uint16_t* codeA;  // [t][R2][SA] q | q1 << 4 | (sign == +1) << 15
-  const uint16_t* codeB;
-  const uint32_t* cutA;   // [t][R2][513] first-pass owner ranges
-  const uint32_t* cutB;
-  const int* scale_exp;   // per absolute inner index (FFT)
-  const double2* tw;      // w_b^j
-  void* partial;          // [g][t][b] double2 (FFT) / double (FWHT)
+  const void* matA;  // [t][kk][R2][SA]
+  const void* matB;
+  const void* codeA;  // [t][R2][SA]
+  const void* codeB;
+  const uint32_t* countA;  // [t][R2][513] cut offsets
+  const uint32_t* countB;
+  const int* scale_exp;
+  const double2* tw;  // w_b^j
+  void* partial;      // [g][t][b] double2 (FFT) / double (FWHT)
   int64_t SA, SB, kc, k0;
   int d, log2b, logR1, logR2, G, accumulate;
 };
 
 // Staged slot e of a segment sits at e + e / 16 (8-byte values) or e + e / 8
-// (4-byte values): every thread reads its own contiguous range, and the
-// spare slots spread neighbouring threads' reads over the banks.
+// (4-byte values): neighbouring threads' ranges start a few slots apart, and
+// the spare slots spread their same-index reads over the banks.
 __host__ __device__ constexpr int64_t spad_len_n(int64_t n, size_t real) {
   return n + n / (real == 8 ? 16 : 8) + 1;
 }
@@ -154,13 +150,13 @@ __host__ __device__ inline int cl_pre_hi(int log2b) { return log2b > 9 ? 1 << (l
 // Shared-memory layout of one CTA, shared by the kernel and the host sizing:
 // NB sub-spectrum buffers, then (FFT) the factored post-twiddle tables, the
 // DIF weight tables when R1 > 1, the pass twiddles and w_R1; then the staged
-// row values of this CTA's segments and their codes.
+// row values of this CTA's segments and their premixed codes.
 struct ClLayout {
   size_t buf, post, pre, ptw, wr, stage, codes, total;
 };
 __host__ __device__ inline size_t cl_align16(size_t x) { return (x + 15) & ~(size_t)15; }
-__host__ __device__ inline ClLayout cl_layout(bool fft, bool f32, int NB, int R1, int log2b, int64_t SA,
-                                              int64_t SB) {
+__host__ __device__ inline ClLayout cl_layout(bool fft, bool f32, bool u16, int NB, int R1, int log2b,
+                                              int64_t SA, int64_t SB) {
   const size_t real = f32 ? 4 : 8, cpx = 2 * real;
   const size_t L = (fft && !f32) ? 4096 : 8192;
   auto plen = [](size_t n, size_t es) { return es == 4 ? n + n / 32 : n + n / 16; };
@@ -179,7 +175,7 @@ __host__ __device__ inline ClLayout cl_layout(bool fft, bool f32, int NB, int R1
   o.stage = p;
   p += cl_align16((size_t)(spad_len_n(SA, real) + spad_len_n(SB, real)) * real);
   o.codes = p;
-  p += cl_align16((size_t)(SA + SB) * 2);
+  p += cl_align16((size_t)(SA + SB) * (u16 ? 2 : 4));
   o.total = p;
   return o;
 }
@@ -196,17 +192,15 @@ static __device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc) {
 }
 static __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// VARIANT 0 = FFT, 1 = FWHT; Real = double (plain) or float (mixed FFT);
-// NB = 2 double-buffers the sub-spectra (one cluster barrier per inner
-// index), NB = 1 when two buffers do not fit in shared memory (two barriers).
-template <int VARIANT, typename Real, int NB>
+// VARIANT 0 = FFT, 1 = FWHT; Real = double (plain) or float (mixed); NB = 2
+// double-buffers the sub-spectra (one cluster barrier per inner index), NB = 1
+// when two buffers do not fit in shared memory (two barriers).
+template <int VARIANT, typename Real, typename CodeT, int NB>
 __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
   constexpr bool kFFT = VARIANT == kVariantFFT;
   constexpr bool kF32 = sizeof(Real) == 4;
   constexpr int LOGL = (kFFT && !kF32) ? 12 : 13;
   constexpr int L = 1 << LOGL;
-  constexpr int QB = LOGL - 9;  // first-pass points per thread: QN = L / kCT
-  constexpr int QN = 1 << QB;
   using C = typename std::conditional<kF32, float2, double2>::type;
   constexpr int ES = kFFT ? (int)sizeof(C) : (int)sizeof(Real);  // shared element size
   constexpr int PL = phys_len<ES>(L);
@@ -214,14 +208,14 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
 
   extern __shared__ __align__(16) unsigned char sm[];
   cg::cluster_group cluster = cg::this_cluster();
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int R1 = 1 << a.logR1, R2 = 1 << a.logR2;
   const int r2 = (int)cluster.block_rank();
   const int logM = a.log2b - a.logR1;  // M = b / R1
   const double2* tw = a.tw;
 
   // ---- shared layout (cl_layout)
-  const ClLayout lay = cl_layout(kFFT, kF32, NB, R1, a.log2b, a.SA, a.SB);
+  const ClLayout lay = cl_layout(kFFT, kF32, sizeof(CodeT) == 2, NB, R1, a.log2b, a.SA, a.SB);
   C* buf0 = reinterpret_cast<C*>(sm + lay.buf);        // FFT: NB x PL complex
   Real* xs0 = reinterpret_cast<Real*>(sm + lay.buf);   // FWHT: NB x (x: PL, y: PL) real
   C* postLo = reinterpret_cast<C*>(sm + lay.post);     // FFT: w_M^{n r2} = postHi[n >> 7] postLo[n & 127]
@@ -233,8 +227,8 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
   Real* wRy = wRx + 16;
   Real* stA = reinterpret_cast<Real*>(sm + lay.stage);  // staged row values, this CTA's segments
   Real* stB = stA + spad_len<Real>(a.SA);
-  uint16_t* cA = reinterpret_cast<uint16_t*>(sm + lay.codes);
-  uint16_t* cB = cA + a.SA;
+  CodeT* cA = reinterpret_cast<CodeT*>(sm + lay.codes);
+  CodeT* cB = cA + a.SA;
 
   // ---- tables (constant over k)
   if (kFFT) {
@@ -284,6 +278,18 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
     }
   }
   auto post = [&](int n) -> C { return cmul(postHi[n >> 7], postLo[n & 127]); };
+  // B fragments of H16 for the FP32 FWHT
+  uint32_t hb[2][2] = {{0u, 0u}, {0u, 0u}};
+  if (!kFFT && kF32) {
+    const int gq = lane >> 2, tq = lane & 3;
+#pragma unroll
+    for (int hf = 0; hf < 2; ++hf) {
+      const int c = gq + 8 * hf;
+      auto hv = [](int e, int cc) { return (__popc(e & cc) & 1) ? -1.f : 1.f; };
+      hb[hf][0] = bf16x2(hv(2 * tq, c), hv(2 * tq + 1, c));
+      hb[hf][1] = bf16x2(hv(2 * tq + 8, c), hv(2 * tq + 9, c));
+    }
+  }
 
   unsigned step = 0;  // inner indices processed by this CTA (selects the buffer)
   // ---- persistent loop over work items (r1, t, k-group); every CTA of a
@@ -294,24 +300,22 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
   const int t = (item >> a.logR1) % a.d;
   const int g = (item >> a.logR1) / a.d;
   __syncthreads();  // the previous item is done with the shared codes and staged rows
-  // codes of this CTA's segments with the DIF weight index of r1 in place
-  // of q1: q | w << 4 | (sign == +1) << 15
+  // codes of this CTA's segment, premixed with the DIF weight index for r1
   {
-    const uint16_t* gA = a.codeA + ((size_t)t * R2 + r2) * a.SA;
-    const uint16_t* gB = a.codeB + ((size_t)t * R2 + r2) * a.SB;
+    const CodeT* gA = reinterpret_cast<const CodeT*>(a.codeA) + ((size_t)t * R2 + r2) * a.SA;
+    const CodeT* gB = reinterpret_cast<const CodeT*>(a.codeB) + ((size_t)t * R2 + r2) * a.SB;
     for (int64_t e = tid; e < a.SA + a.SB; e += kCT) {
-      const uint32_t c = e < a.SA ? (uint32_t)gA[e] : (uint32_t)gB[e - a.SA];
-      const uint32_t q1 = (c >> 4) & 0x7ffu;
+      const uint32_t h = e < a.SA ? (uint32_t)gA[e] : (uint32_t)gB[e - a.SA];
+      const uint32_t m = h & (L - 1), q1 = h >> LOGL;
       const uint32_t w = kFFT ? ((q1 * (uint32_t)r1) & (uint32_t)(R1 - 1)) : (__popc(q1 & (uint32_t)r1) & 1u);
-      (e < a.SA ? cA[e] : cB[e - a.SA]) = (uint16_t)((c & 0x800fu) | (w << 4));
+      (e < a.SA ? cA[e] : cB[e - a.SA]) = (CodeT)(m | (w << LOGL));
     }
   }
-  const uint32_t* cutA = a.cutA + ((size_t)t * R2 + r2) * (kCT + 1);
-  const uint32_t* cutB = a.cutB + ((size_t)t * R2 + r2) * (kCT + 1);
+  // this thread's contiguous slot range in its segment (compact plan)
+  const uint32_t* cutA = a.countA + ((size_t)t * R2 + r2) * (kCT + 1);
+  const uint32_t* cutB = a.countB + ((size_t)t * R2 + r2) * (kCT + 1);
   const int begA = (int)cutA[tid], endA = (int)cutA[tid + 1];
   const int begB = (int)cutB[tid], endB = (int)cutB[tid + 1];
-  const uint32_t* srcA = a.srcA + ((size_t)t * R2 + r2) * a.SA;
-  const uint32_t* srcB = a.srcB + ((size_t)t * R2 + r2) * a.SB;
 
   // ---- accumulators for this CTA's outputs
   // group gi = tid + 512 u (u < OUT / 8) covers sub-spectrum position
@@ -362,41 +366,18 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
       while (k < ke && __ldg(a.scale_exp + a.k0 + k) == kCSkip) ++k;
     return k;
   };
-  // gather this CTA's segments of row k into the staging area in slot
-  // order (thread i copies slots i, i + 512, ...: the index loads are
-  // coalesced; four are loaded before their copies are issued)
+  // stage this CTA's segments of row k, coalesced (thread i copies slots i,
+  // i + 512, ...); the copies land before the barrier that precedes the
+  // scatter, and are issued after the barrier that ends the previous scatter
   const int totA = (int)cutA[kCT], totB = (int)cutB[kCT];
-  auto gather = [&](const Real* row, const uint32_t* src, Real* st, int tot) {
-    for (int e0 = tid; e0 < tot; e0 += 4 * kCT) {
-      uint32_t ix[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) ix[u] = e0 + u * kCT < tot ? __ldg(src + e0 + u * kCT) : 0u;
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int e = e0 + u * kCT;
-        if (e < tot) {
-          if (kF32) cp_async4(st + spad<Real>(e), row + (ix[u] & 0x7fffffffu));
-          else cp_async8(st + spad<Real>(e), row + (ix[u] & 0x7fffffffu));
-        }
-      }
-    }
-  };
-  // copied rows: this CTA's segments of row k are contiguous (thread i
-  // copies slots i, i + 512, ...)
-  auto copy = [&](const Real* seg, Real* st, int tot) {
-    for (int e = tid; e < tot; e += kCT) {
-      if (kF32) cp_async4(st + spad<Real>(e), seg + e);
-      else cp_async8(st + spad<Real>(e), seg + e);
-    }
-  };
-  const bool copied = a.matA != nullptr;
   auto stage = [&](int64_t k) {
-    if (copied) {
-      copy(reinterpret_cast<const Real*>(a.matA) + (((size_t)t * a.kc + k) * R2 + r2) * a.SA, stA, totA);
-      copy(reinterpret_cast<const Real*>(a.matB) + (((size_t)t * a.kc + k) * R2 + r2) * a.SB, stB, totB);
-    } else {
-      gather(reinterpret_cast<const Real*>(a.A) + (size_t)(a.k0 + k) * (size_t)a.lda, srcA, stA, totA);
-      gather(reinterpret_cast<const Real*>(a.B) + (size_t)(a.k0 + k) * (size_t)a.ldb, srcB, stB, totB);
+    const Real* rA = reinterpret_cast<const Real*>(a.matA) + (((size_t)t * a.kc + k) * R2 + r2) * a.SA;
+    const Real* rB = reinterpret_cast<const Real*>(a.matB) + (((size_t)t * a.kc + k) * R2 + r2) * a.SB;
+    for (int e = tid; e < totA; e += kCT) {
+      if (kF32) cp_async4(stA + spad<Real>(e), rA + e); else cp_async8(stA + spad<Real>(e), rA + e);
+    }
+    for (int e = tid; e < totB; e += kCT) {
+      if (kF32) cp_async4(stB + spad<Real>(e), rB + e); else cp_async8(stB + spad<Real>(e), rB + e);
     }
   };
   int64_t kk = next_k(kb);
@@ -414,96 +395,117 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
     C* buf = buf0 + (NB == 2 ? (size_t)(step & 1) * PL : 0);
     Real* xs = xs0 + (NB == 2 ? (size_t)(step & 1) * 2 * PL : 0);
     Real* ys = xs + PL;
+    if (kFFT) {
+      for (int e = tid; e < PL; e += kCT) buf[e] = mk((Real)0, (Real)0);
+    } else {
+      for (int e = tid; e < PL; e += kCT) { xs[e] = (Real)0; ys[e] = (Real)0; }
+    }
     cp_async_wait_all();  // this thread's copies of row kk; the barrier publishes all
     __syncthreads();
-
-    // ---- count sketch of this thread's slots, summed into the registers
-    // of its first-pass butterfly: element q of acc is sub-bucket
-    // owner-point q.  Slots are sorted by q, so the unrolled q loop keeps
-    // the register index static.  The scale is a power of two, applied per
-    // value.  FFT with R1 <= 2 (real DIF weights +-1): side A adds to the
-    // real parts, side B to the imaginary parts; R1 = 4 uses (-i)^w
-    // exactly, larger R1 the table w_R1; side B adds i times its value.
-    C acc[QN];
-    Real ya[QN];  // FWHT: side B sums (side A in acc[].x)
-#pragma unroll
-    for (int q = 0; q < QN; ++q) {
-      acc[q] = mk((Real)0, (Real)0);
-      if (!kFFT) ya[q] = (Real)0;
-    }
+    // ---- scatter this CTA's residue segment.  The plan cuts the segment at
+    // bucket boundaries, so every bucket has one writer thread; its slots are
+    // sorted by bucket.  Per batch of kCBatch slots a thread loads every
+    // target first, sums runs of equal buckets in registers and stores once
+    // per run.  The scale is a power of two, applied per value.  Side A and
+    // side B write different words when the DIF weights are real (FFT with
+    // R1 <= 2: real / imaginary part; FWHT: x / y), so both sides run at once.
+    const bool split = !kFFT || R1 <= 2;
 #pragma unroll
     for (int side = 0; side < 2; ++side) {
       const Real* st = side == 0 ? stA : stB;
-      const uint16_t* codes = side == 0 ? cA : cB;
-      const int end = side == 0 ? endA : endB;
+      const CodeT* codes = side == 0 ? cA : cB;
+      const int beg = side == 0 ? begA : begB, end = side == 0 ? endA : endB;
       const Real sc = side == 0 ? alpha : beta;
-      int s = side == 0 ? begA : begB;
-      uint32_t c = s < end ? (uint32_t)codes[s] : 0u;
+      Real* words = kFFT ? reinterpret_cast<Real*>(buf) + side : (side == 0 ? xs : ys);
+      constexpr int kWordStride = kFFT ? 2 : 1;  // Real words per element
+      for (int s0 = beg; s0 < end; s0 += kCBatch) {
+        Real cx[kCBatch], cy[kCBatch];
+        int pp[kCBatch];
+        uint32_t mm[kCBatch];
 #pragma unroll
-      for (int q = 0; q < QN; ++q) {
-        while (s < end && (int)(c & 15u) == q) {
-          Real v = st[spad<Real>(s)] * sc;
-          if (!copied && !(c >> 15)) v = -v;  // copied rows carry their sign
-          const uint32_t w = (c >> 4) & 0x7ffu;
-          if constexpr (!kFFT) {
-            if (w) v = -v;
-            if (side == 0) acc[q].x += v;
-            else ya[q] += v;
-          } else if (a.logR1 <= 1) {
-            if (w & 1u) v = -v;
-            if (side == 0) acc[q].x += v;
-            else acc[q].y += v;
+        for (int u = 0; u < kCBatch; ++u) {
+          const int e = s0 + u;
+          const bool ok = e < end;
+          const Real v = ok ? st[spad<Real>(e)] * sc : (Real)0;
+          const uint32_t h = ok ? (uint32_t)codes[e] : 0u;
+          const uint32_t m = h & (L - 1), w = h >> LOGL;
+          mm[u] = ok ? m : 0xffffffffu;
+          pp[u] = phys<ES>(kFFT ? (int)(__brev(m) >> (32 - LOGL)) : (int)m);
+          if (!kFFT) {
+            cx[u] = w ? -v : v;
+            cy[u] = (Real)0;
+          } else if (split) {
+            cx[u] = (w & 1u) ? -v : v;  // w_2^w = +-1 (w = 0 when R1 = 1)
+            cy[u] = (Real)0;
+          } else if (a.logR1 == 2) {  // w_4^w = (-i)^w exactly
+            cx[u] = (w & 1u) ? (Real)0 : ((w & 2u) ? -v : v);
+            cy[u] = (w & 1u) ? ((w & 2u) ? v : -v) : (Real)0;
           } else {
-            Real cx, cy;
-            if (a.logR1 == 2) {  // w_4^w = (-i)^w exactly
-              cx = (w & 1u) ? (Real)0 : ((w & 2u) ? -v : v);
-              cy = (w & 1u) ? ((w & 2u) ? v : -v) : (Real)0;
-            } else {
-              cx = v * wRx[w];
-              cy = v * wRy[w];
-            }
-            if (side == 0) acc[q] = mk(acc[q].x + cx, acc[q].y + cy);
-            else acc[q] = mk(acc[q].x - cy, acc[q].y + cx);
+            cx[u] = v * wRx[w];
+            cy[u] = v * wRy[w];
           }
-          ++s;
-          c = s < end ? (uint32_t)codes[s] : 0u;
+          if (kFFT && !split && side == 1) {  // side B adds i c
+            const Real tx = cx[u];
+            cx[u] = -cy[u];
+            cy[u] = tx;
+          }
+        }
+        if (split) {
+          Real old[kCBatch];
+#pragma unroll
+          for (int u = 0; u < kCBatch; ++u) old[u] = mm[u] != 0xffffffffu ? words[pp[u] * kWordStride] : (Real)0;
+          Real rx = (Real)0;
+#pragma unroll
+          for (int u = 0; u < kCBatch; ++u) {
+            rx = (u > 0 && mm[u] == mm[u - 1]) ? rx + cx[u] : cx[u];
+            const bool last = u == kCBatch - 1 || mm[u + 1] != mm[u];
+            if (mm[u] != 0xffffffffu && last) words[pp[u] * kWordStride] = old[u] + rx;
+          }
+        } else {
+          C old[kCBatch];
+#pragma unroll
+          for (int u = 0; u < kCBatch; ++u) old[u] = mm[u] != 0xffffffffu ? buf[pp[u]] : mk((Real)0, (Real)0);
+          Real rx = (Real)0, ry = (Real)0;
+#pragma unroll
+          for (int u = 0; u < kCBatch; ++u) {
+            const bool cont = u > 0 && mm[u] == mm[u - 1];
+            rx = cont ? rx + cx[u] : cx[u];
+            ry = cont ? ry + cy[u] : cy[u];
+            const bool last = u == kCBatch - 1 || mm[u + 1] != mm[u];
+            if (mm[u] != 0xffffffffu && last) buf[pp[u]] = mk(old[u].x + rx, old[u].y + ry);
+          }
         }
       }
+      if (side == 0 && !split) __syncthreads();
     }
+    __syncthreads();         // the scatter is done with the staged row
+    if (kn < ke) stage(kn);  // overlaps the transform and the combine
 
-    // ---- first pass from registers, then the remaining passes of the local
-    // transform of length L (results stay in shared memory)
+    // ---- local transform of length L (results stay in shared memory)
     if (kFFT && !kF32) {
       // 4 radix-8 DIT passes; pass 0 (constant twiddles) applies the DIF
       // weight w_b^{n1 r1}, pass 3 the post-twiddle w_M^{n r2}
-      {
-        const int base = tid * 8;
-        C x[8];
 #pragma unroll
-        for (int e = 0; e < 8; ++e) x[e] = acc[brev_bits<3>(e)];
-        if (R1 > 1) {
-#pragma unroll
-          for (int e = 0; e < 8; ++e) {
-            const uint32_t m = __brev((uint32_t)(base + e)) >> (32 - LOGL);
-            const uint32_t xx = ((m << a.logR2) + (uint32_t)r2) * (uint32_t)r1;  // n1 r1 < b
-            x[e] = cmul(x[e], cmul(preHi[xx >> 9], preLo[xx & 511]));
-          }
-        }
-        r8_first(x);
-#pragma unroll
-        for (int e = 0; e < 8; ++e) buf[phys<ES>(base + e)] = x[e];
-      }
-      __syncthreads();         // the sketch is done with the staged row; pass 0 is written
-      if (kn < ke) stage(kn);  // overlaps the transform and the combine
-#pragma unroll
-      for (int ps = 1; ps < 4; ++ps) {
+      for (int ps = 0; ps < 4; ++ps) {
         const int s0 = 3 * ps, half = 1 << s0;
         const int kk2 = tid & (half - 1);
         const int base = ((tid >> s0) << (s0 + 3)) | kk2;
         C x[8];
 #pragma unroll
         for (int e = 0; e < 8; ++e) x[e] = buf[phys<ES>(base + e * half)];
-        r8(x, ptw[(ps == 1 ? 0 : (ps == 2 ? 8 : 72)) + kk2]);
+        if (ps == 0) {
+          if (R1 > 1) {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+              const uint32_t m = __brev((uint32_t)(base + e)) >> (32 - LOGL);
+              const uint32_t xx = ((m << a.logR2) + (uint32_t)r2) * (uint32_t)r1;  // n1 r1 < b
+              x[e] = cmul(x[e], cmul(preHi[xx >> 9], preLo[xx & 511]));
+            }
+          }
+          r8_first(x);
+        } else {
+          r8(x, ptw[(ps == 1 ? 0 : (ps == 2 ? 8 : 72)) + kk2]);
+        }
         if (ps == 3) {
 #pragma unroll
           for (int e = 0; e < 8; ++e) x[e] = cmul(x[e], post(base + e * half));
@@ -513,12 +515,12 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
         if (ps < 3) __syncthreads();
       }
     } else if (kFFT) {
-      // FP32, L = 8192: radix-16 (stages 0-3) from registers + 3 radix-8 passes
+      // FP32, L = 8192: radix-16 (stages 0-3) + 3 radix-8 passes
       {
         const int base = tid * 16;
         C x[16];
 #pragma unroll
-        for (int e = 0; e < 16; ++e) x[e] = acc[brev_bits<4>(e)];
+        for (int e = 0; e < 16; ++e) x[e] = buf[phys<ES>(base + e)];
         if (R1 > 1) {
 #pragma unroll
           for (int e = 0; e < 16; ++e) {
@@ -549,7 +551,6 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
         for (int e = 0; e < 16; ++e) buf[phys<ES>(base + e)] = x[e];
       }
       __syncthreads();
-      if (kn < ke) stage(kn);
 #pragma unroll
       for (int ps = 1; ps <= 3; ++ps) {
         const int s0 = ps == 1 ? 4 : (ps == 2 ? 7 : 10), half = 1 << s0;
@@ -571,21 +572,19 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
         }
         if (ps < 3) __syncthreads();
       }
-    } else {
-      // FP64 WHT of x and y: radix-16 from registers + 3 radix-8 passes,
-      // natural order
+    } else if (!kF32) {
+      // FP64 WHT of x and y: radix-16 + 3 radix-8 passes, natural order
       {
         const int base = tid * 16;
         Real x[16], y[16];
 #pragma unroll
-        for (int e = 0; e < 16; ++e) { x[e] = acc[e].x; y[e] = ya[e]; }
+        for (int e = 0; e < 16; ++e) { x[e] = xs[phys<ES>(base + e)]; y[e] = ys[phys<ES>(base + e)]; }
         whtr<Real, 16>(x);
         whtr<Real, 16>(y);
 #pragma unroll
         for (int e = 0; e < 16; ++e) { xs[phys<ES>(base + e)] = x[e]; ys[phys<ES>(base + e)] = y[e]; }
       }
       __syncthreads();
-      if (kn < ke) stage(kn);
 #pragma unroll
       for (int ps = 1; ps <= 3; ++ps) {
         const int s0 = ps == 1 ? 4 : (ps == 2 ? 7 : 10), half = 1 << s0;
@@ -602,6 +601,27 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
           for (int e = 0; e < 8; ++e) { xs[phys<ES>(base + e * half)] = x[e]; ys[phys<ES>(base + e * half)] = y[e]; }
         }
         if (ps < 3) __syncthreads();
+      }
+    } else {
+      // FP32 WHT: three Hadamard-16 factors on the tensor cores + radix-2
+      float* fx = reinterpret_cast<float*>(xs);
+      float* fy = reinterpret_cast<float*>(ys);
+      h16<0>(fx, hb, warp, lane);
+      h16<0>(fy, hb, warp, lane);
+      __syncthreads();
+      h16<1>(fx, hb, warp, lane);
+      h16<1>(fy, hb, warp, lane);
+      __syncthreads();
+      h16<2>(fx, hb, warp, lane);
+      h16<2>(fy, hb, warp, lane);
+      __syncthreads();
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const int m = tid + kCT * e;
+        const float x0 = fx[phys<ES>(m)], x1 = fx[phys<ES>(m + 4096)];
+        const float y0 = fy[phys<ES>(m)], y1 = fy[phys<ES>(m + 4096)];
+        fx[phys<ES>(m)] = x0 + x1; fx[phys<ES>(m + 4096)] = x0 - x1;
+        fy[phys<ES>(m)] = y0 + y1; fy[phys<ES>(m + 4096)] = y0 - y1;
       }
     }
 
@@ -621,7 +641,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
         if (R2 == 16) {
           const int rb = half ? 8 : 0;
 #pragma unroll
-          for (int r = 0; r < 8; ++r) z[r] = remote(buf, rb + r, phys<ES>(n));
+          for (int r = 0; r < 8; ++r) z[r] = cluster.map_shared_rank(buf, rb + r)[phys<ES>(n)];
 #pragma unroll
           for (int r = 0; r < 8; ++r) {
             const C o = mk(__shfl_xor_sync(0xffffffffu, z[r].x, 1), __shfl_xor_sync(0xffffffffu, z[r].y, 1));
@@ -631,7 +651,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
           }
         } else {
 #pragma unroll
-          for (int r = 0; r < 8; ++r) z[r] = remote(buf, r, phys<ES>(n));
+          for (int r = 0; r < 8; ++r) z[r] = cluster.map_shared_rank(buf, r)[phys<ES>(n)];
         }
         dft8(z);
 #pragma unroll
@@ -653,8 +673,8 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
           const int rb = half ? 8 : 0;
 #pragma unroll
           for (int r = 0; r < 8; ++r) {
-            zx[r] = remote(xs, rb + r, phys<ES>(n));
-            zy[r] = remote(ys, rb + r, phys<ES>(n));
+            zx[r] = cluster.map_shared_rank(xs, rb + r)[phys<ES>(n)];
+            zy[r] = cluster.map_shared_rank(ys, rb + r)[phys<ES>(n)];
           }
 #pragma unroll
           for (int r = 0; r < 8; ++r) {
@@ -665,8 +685,8 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
         } else {
 #pragma unroll
           for (int r = 0; r < 8; ++r) {
-            zx[r] = remote(xs, r, phys<ES>(n));
-            zy[r] = remote(ys, r, phys<ES>(n));
+            zx[r] = cluster.map_shared_rank(xs, r)[phys<ES>(n)];
+            zy[r] = cluster.map_shared_rank(ys, r)[phys<ES>(n)];
           }
         }
         whtr<Real, 8>(zx);
@@ -674,7 +694,8 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
 #pragma unroll
         for (int jj = 0; jj < 8; ++jj) {
           const int o = u * 8 + jj;
-          qd[o][0] = fma((double)zx[jj], (double)zy[jj], qd[o][0]);
+          if (kF32) tsum(qh[o][0], ql[o][0], (float)(zx[jj] * zy[jj]));
+          else qd[o][0] = fma((double)zx[jj], (double)zy[jj], qd[o][0]);
         }
       }
     }
@@ -697,97 +718,83 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
 }
 
 // ------------------------------------------------------------------ host
-// Where the staged rows come from: gathered from AT and B in place
-// (CMM_CLUSTER_ROWS=gather), or copied first, per chunk of inner indices, into
-// plan order with the sign applied (copy, the default).
-bool cluster_rows_gathered() {
-  static const bool g = [] {
-    const char* e = getenv("CMM_CLUSTER_ROWS");
-    return e && !strcmp(e, "gather");
-  }();
-  return g;
-}
-
-int cluster_log_slab(int variant, bool f32) { return (variant == kVariantFFT && !f32) ? 12 : 13; }
+static int cl_logL(int variant, bool f32) { return (variant == kVariantFFT && !f32) ? 12 : 13; }
 
 bool sketch_cluster_applicable(int variant, bool f32, int b) {
-  if (variant == kVariantFWHT && f32) return false;  // mixed FWHT: tensor-core slab kernel
+  const int logL = cl_logL(variant, f32);
   int log2b = 0;
   while ((1 << log2b) < b) ++log2b;
-  // R = b / L >= 8; the DIF twiddle table covers b <= 2^19
-  return log2b - cluster_log_slab(variant, f32) >= 3 && log2b <= 19;
+  return log2b - logL >= 3 && log2b <= 19;  // R >= 8; DIF twiddle table covers b <= 2^19
 }
 
 constexpr size_t kClSmemMax = 227 * 1024;
 
-template <int V, typename Real, int NB>
+template <int V, typename Real, typename CodeT, int NB>
 static void cl_kernel_attrs(size_t smem) {
-  auto k = k_sketch_cluster<V, Real, NB>;
+  auto k = k_sketch_cluster<V, Real, CodeT, NB>;
   CMM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   CMM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
 }
 
 // shared bytes of one CTA and the buffer count: two sub-spectrum buffers
 // when they fit, else one
-static size_t cl_smem(int variant, bool f32, int R1, int log2b, int64_t SA, int64_t SB, int* nb) {
+static size_t cl_smem(int variant, bool f32, bool u16, int R1, int log2b, int64_t SA, int64_t SB, int* nb) {
   const bool fft = variant == kVariantFFT;
-  const size_t two = cl_layout(fft, f32, 2, R1, log2b, SA, SB).total;
+  const size_t two = cl_layout(fft, f32, u16, 2, R1, log2b, SA, SB).total;
   if (two <= kClSmemMax) {
     if (nb) *nb = 2;
     return two;
   }
   if (nb) *nb = 1;
-  return cl_layout(fft, f32, 1, R1, log2b, SA, SB).total;
+  return cl_layout(fft, f32, u16, 1, R1, log2b, SA, SB).total;
 }
 
-static cudaLaunchConfig_t cluster_config(dim3 grid, int threads, int R2, size_t smem, cudaStream_t s,
-                                         cudaLaunchAttribute* attr) {
+template <int V, typename Real, typename CodeT, int NB>
+static void cl_launch(const ClArgs& a, dim3 grid, int R2, size_t smem, cudaStream_t s) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
-  cfg.blockDim = dim3((unsigned)threads, 1, 1);
+  cfg.blockDim = dim3(kCT, 1, 1);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
+  cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
   attr[0].val.clusterDim.x = (unsigned)R2;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cfg;
+  CMM_CUDA(cudaLaunchKernelEx(&cfg, k_sketch_cluster<V, Real, CodeT, NB>, a));
 }
 
-template <typename K>
-static int max_clusters_of(K kernel, int threads, int R2, size_t smem) {
+template <int V, typename Real, typename CodeT>
+static int cl_max_clusters(int R2, size_t smem) {
+  cl_kernel_attrs<V, Real, CodeT, 1>(smem);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)R2, 1, 1);
+  cfg.blockDim = dim3(kCT, 1, 1);
+  cfg.dynamicSmemBytes = smem;
   cudaLaunchAttribute attr[1];
-  cudaLaunchConfig_t cfg = cluster_config(dim3((unsigned)R2, 1, 1), threads, R2, smem, nullptr, attr);
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)R2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
   int n = 0;
-  if (cudaOccupancyMaxActiveClusters(&n, kernel, &cfg) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveClusters(&n, k_sketch_cluster<V, Real, CodeT, 1>, &cfg) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
   return n;
 }
 
-static int cl_max_clusters(int variant, bool f32, int R2, size_t smem) {
-  if (variant == kVariantFFT && f32) {
-    cl_kernel_attrs<0, float, 1>(smem);
-    return max_clusters_of(k_sketch_cluster<0, float, 1>, kCT, R2, smem);
-  }
-  if (variant == kVariantFFT) {
-    cl_kernel_attrs<0, double, 1>(smem);
-    return max_clusters_of(k_sketch_cluster<0, double, 1>, kCT, R2, smem);
-  }
-  cl_kernel_attrs<1, double, 1>(smem);
-  return max_clusters_of(k_sketch_cluster<1, double, 1>, kCT, R2, smem);
-}
-
 // Chooses R2 in {16, 8} and the k-group count G from the number of
 // co-resident clusters NC: the grid holds NC persistent clusters that share
 // the R1 * d * G work items round-robin; the estimate ceil(items/NC)/G is
 // minimised (ties to R2 = 16: less scatter redundancy, fewer items).
-ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, int64_t n_max) {
+ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, int64_t est_slots) {
   ClusterPlan C;
-  C.logL = cluster_log_slab(variant, f32);
+  C.logL = cl_logL(variant, f32);
   C.log2b = 0;
   while ((1 << C.log2b) < b) ++C.log2b;
   const int logR = C.log2b - C.logL;
@@ -795,11 +802,12 @@ ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, i
   for (int logR2 : {4, 3}) {
     if (logR2 > logR) continue;
     const int R2 = 1 << logR2, R1 = 1 << (logR - logR2);
-    // expected largest residue segment: n / R2 plus a margin for the spread
-    const int64_t est_slots = (n_max + R2 - 1) / R2 + (n_max + R2 - 1) / R2 / 8 + 64;
-    const size_t smem = cl_smem(variant, f32, R1, C.log2b, est_slots, est_slots, nullptr);
-    if (smem > kClSmemMax) continue;
-    const int mx = cl_max_clusters(variant, f32, R2, smem);
+    const size_t smem = cl_smem(variant, f32, true, R1, C.log2b, est_slots, est_slots, nullptr);
+    int mx;
+    if (variant == kVariantFFT)
+      mx = f32 ? cl_max_clusters<0, float, uint16_t>(R2, smem) : cl_max_clusters<0, double, uint16_t>(R2, smem);
+    else
+      mx = f32 ? cl_max_clusters<1, float, uint16_t>(R2, smem) : cl_max_clusters<1, double, uint16_t>(R2, smem);
     if (mx <= 0) continue;
     const int64_t base = (int64_t)R1 * d;
     for (int64_t G = 1; G <= 64; ++G) {
@@ -826,27 +834,20 @@ ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, i
 }
 
 bool cluster_smem_fits(int variant, bool f32, const ClusterPlan& C, const SlabPlan& P) {
-  return cl_smem(variant, f32, 1 << C.logR1, C.log2b, P.EA, P.EB, nullptr) <= kClSmemMax;
+  return cl_smem(variant, f32, P.u16, 1 << C.logR1, C.log2b, P.EA, P.EB, nullptr) <= kClSmemMax;
 }
 
-void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const SlabPlan& P, const void* dA,
-                           const void* dB, const void* dMatA, const void* dMatB, int64_t kc,
-                           const int* dScaleExp, int64_t k0, const double2* dTw, void* dPartial, int d,
-                           int accumulate, cudaStream_t s) {
-  if (!P.owner || P.logL != C.logL) throw runtime_error("cluster sketch: plan does not match the kernel");
+void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const SlabPlan& P,
+                           const void* dMatA, const void* dMatB, int64_t kc, const int* dScaleExp,
+                           int64_t k0, const double2* dTw, void* dPartial, int d, int accumulate,
+                           cudaStream_t s) {
   ClArgs a;
-  a.A = dA;
-  a.B = dB;
   a.matA = dMatA;
   a.matB = dMatB;
-  a.lda = P.n_a;
-  a.ldb = P.n_b;
-  a.srcA = P.srcA.as<uint32_t>();
-  a.srcB = P.srcB.as<uint32_t>();
-  a.codeA = P.codeA.as<uint16_t>();
-  a.codeB = P.codeB.as<uint16_t>();
-  a.cutA = P.countA.as<uint32_t>();
-  a.cutB = P.countB.as<uint32_t>();
+  a.codeA = P.codeA.ptr;
+  a.codeB = P.codeB.ptr;
+  a.countA = P.countA.as<uint32_t>();
+  a.countB = P.countB.as<uint32_t>();
   a.scale_exp = dScaleExp;
   a.tw = dTw;
   a.partial = dPartial;
@@ -862,32 +863,30 @@ void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const Sl
   a.accumulate = accumulate;
   const int R2 = 1 << C.logR2, R1 = 1 << C.logR1;
   int nb = 1;
-  const size_t smem = cl_smem(variant, f32, R1, C.log2b, a.SA, a.SB, &nb);
+  const size_t smem = cl_smem(variant, f32, P.u16, R1, C.log2b, a.SA, a.SB, &nb);
   if (smem > kClSmemMax) throw unsupported("cluster sketch: residue segments too large for shared memory");
   if (getenv("CMM_DEBUG"))
-    fprintf(stderr, "[cmm] cluster launch: smem=%zu buffers=%d SA=%lld SB=%lld rows=%s\n", smem, nb,
-            (long long)a.SA, (long long)a.SB, dMatA ? "copied" : "gathered");
+    fprintf(stderr, "[cmm] cluster launch: smem=%zu buffers=%d SA=%lld SB=%lld\n", smem, nb, (long long)a.SA,
+            (long long)a.SB);
   const dim3 grid((unsigned)R2, (unsigned)C.max_clusters, 1);
   ProfScope prof("sketch", s);
   count_launch();
-  cudaLaunchAttribute attr[1];
-  const cudaLaunchConfig_t cfg = cluster_config(grid, kCT, R2, smem, s, attr);
-#define CMM_CL(V, T)                                                   \
-  do {                                                                 \
-    if (nb == 2) {                                                     \
-      cl_kernel_attrs<V, T, 2>(smem);                                  \
-      CMM_CUDA(cudaLaunchKernelEx(&cfg, k_sketch_cluster<V, T, 2>, a)); \
-    } else {                                                           \
-      cl_kernel_attrs<V, T, 1>(smem);                                  \
-      CMM_CUDA(cudaLaunchKernelEx(&cfg, k_sketch_cluster<V, T, 1>, a)); \
-    }                                                                  \
+#define CMM_CL(V, T, CT)                                  \
+  do {                                                     \
+    if (nb == 2) {                                         \
+      cl_kernel_attrs<V, T, CT, 2>(smem);                  \
+      cl_launch<V, T, CT, 2>(a, grid, R2, smem, s);        \
+    } else {                                               \
+      cl_kernel_attrs<V, T, CT, 1>(smem);                  \
+      cl_launch<V, T, CT, 1>(a, grid, R2, smem, s);        \
+    }                                                      \
   } while (0)
   if (variant == kVariantFFT) {
-    if (f32) CMM_CL(0, float);
-    else CMM_CL(0, double);
+    if (f32) { if (P.u16) CMM_CL(0, float, uint16_t); else CMM_CL(0, float, uint32_t); }
+    else { if (P.u16) CMM_CL(0, double, uint16_t); else CMM_CL(0, double, uint32_t); }
   } else {
-    if (f32) throw unsupported("cluster sketch: FP32 FWHT runs on the slab kernel");
-    CMM_CL(1, double);
+    if (f32) { if (P.u16) CMM_CL(1, float, uint16_t); else CMM_CL(1, float, uint32_t); }
+    else { if (P.u16) CMM_CL(1, double, uint16_t); else CMM_CL(1, double, uint32_t); }
   }
 #undef CMM_CL
   CMM_CUDA(cudaGetLastError());

@@ -10,9 +10,9 @@ kernels (asserted through cmm_last_sketch_kernel) and cover:
   * several work items per cluster and several k-groups;
   * all-zero rows, which every CTA of a cluster skips, including at the
     start and end of the inner range (the staged next row must follow);
-  * chunked launches over streamed host rows (accumulating partials);
-  * the staged rows copied per chunk in slot order (the default) -- run the
-    file with CMM_CLUSTER_ROWS=gather for the in-place gathers.
+  * chunked materialization (accumulating launches), on device inputs and
+    on streamed host rows;
+  * each slot's sign applied once, on rows of very different scales.
 Tolerances: FP64 sketch within 1e-11 * max|p| absolute; mixed within
 2e-5 * max|p|.
 """
@@ -91,11 +91,21 @@ def test_fft_all_rows_zero(gpu, oracle):
     assert float(np.abs(p).max()) == 0.0
 
 
+@pytest.mark.parametrize("variant,b", [("fft", 1 << 16), ("fwht", 1 << 17)])
+def test_chunked_materialization(gpu, oracle, variant, b, monkeypatch):
+    # a small budget runs several materialize + sketch launches that accumulate
+    monkeypatch.setenv("CMM_MATERIALIZE_BYTES", str(300 * 1024))
+    rng = np.random.default_rng(b + 7)
+    AT = rng.standard_normal((64, 400))
+    B = rng.standard_normal((64, 380))
+    check(variant, None, AT, B, 3, b, 21, oracle)
+
+
 @pytest.mark.parametrize("variant,b", [("fft", 1 << 15), ("fwht", 1 << 16)])
 def test_chunked_launches_accumulate(gpu, oracle, variant, b):
-    # the host entry point streams the rows in chunks (an eighth of the inner
-    # range, the first one an eighth of that): several cluster launches,
-    # each adding to the k-group partials of the previous ones
+    # the host entry point streams the rows in chunks (the first one an
+    # eighth of the copy budget): several cluster launches, each adding to
+    # the k-group partials of the previous ones
     rng = np.random.default_rng(b + 7)
     AT = rng.standard_normal((600, 120))
     B = rng.standard_normal((600, 100))
@@ -104,9 +114,9 @@ def test_chunked_launches_accumulate(gpu, oracle, variant, b):
 
 
 def test_unbalanced_rows_and_signs(gpu, oracle):
-    """Each slot's sign is applied once (by the row copy, or per slot when
-    gathering): rows of very different scales in A and B (the FFT row
-    balance) and a planted large entry, both variants."""
+    """Each slot's sign is applied once, by the row copy: rows of very
+    different scales in A and B (the FFT row balance) and a planted large
+    entry, both variants."""
     rng = np.random.default_rng(19)
     AT = rng.standard_normal((50, 333)) * np.logspace(-3, 3, 50)[:, None]
     B = rng.standard_normal((50, 277)) * np.logspace(3, -3, 50)[:, None]

@@ -2,10 +2,8 @@
 the sketch works on earlier chunks of the inner index (a second stream, one
 event per chunk, the FFT row scales computed per chunk).
 
-With a small materialization budget (slab kernels) or by the cluster
-kernels' own chunking (an eighth of the inner range per launch) the
-products below run several chunks through that feed, on every sketch kernel
-family.  Each launch splits its own chunk into k-groups, so the host path
+With a small materialization budget the products below run several chunks
+through that feed, on every sketch kernel family.  Each launch splits its own chunk into k-groups, so the host path
 sums the inner indices in a different grouping than the single launch of
 the device entry point: the two agree within 1e-13 * max|p| (FP64) or
 1e-7 * max|p| (mixed; bit-identical when both run one launch), and both are
