@@ -205,9 +205,12 @@ SlabPlan make_slab_plan(const uint32_t* dCodesA, const uint32_t* dCodesB, int64_
 
 // ---------------------------------------------------------- materialize
 // out[t][kk][e] = sign * row_k[src[t][e]] (0 for padding), for both sides,
-// for inner indices k0 + kk, kk < kc.  One CTA per inner index; the row is
-// staged in shared memory when it fits.
-constexpr int kMatThreads = 512;
+// for inner indices k0 + kk, kk < kc.  One CTA of 1024 threads per inner
+// index; the row is staged in shared memory when it fits.  Each thread
+// writes four consecutive slots (S is a multiple of 8): one 16-byte load of
+// their indices, two 16-byte streaming stores (the copies are read back
+// once, by the sketch kernel).
+constexpr int kMatThreads = 1024;
 
 template <bool STAGE>
 __global__ void __launch_bounds__(kMatThreads) k_materialize(const double* __restrict__ AT,
@@ -231,16 +234,22 @@ __global__ void __launch_bounds__(kMatThreads) k_materialize(const double* __res
       __syncthreads();
     }
     for (int t = 0; t < d; ++t) {
-      const uint32_t* st = src + (size_t)t * S;
-      double* ot = out + ((size_t)t * kc + kk) * S;
-      for (int64_t e = threadIdx.x; e < S; e += kMatThreads) {
-        const uint32_t sv = __ldg(st + e);
-        double v = 0.0;
-        if (sv != kPadSlot) {
-          v = STAGE ? srow[sv & 0x7fffffffu] : __ldg(row + (sv & 0x7fffffffu));
-          if (!(sv >> 31)) v = -v;
+      const uint4* st = reinterpret_cast<const uint4*>(src + (size_t)t * S);
+      double2* ot = reinterpret_cast<double2*>(out + ((size_t)t * kc + kk) * S);
+      for (int64_t q = threadIdx.x; q < S / 4; q += kMatThreads) {
+        const uint4 sv = __ldg(st + q);
+        const uint32_t svs[4] = {sv.x, sv.y, sv.z, sv.w};
+        double v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          v[u] = 0.0;
+          if (svs[u] != kPadSlot) {
+            v[u] = STAGE ? srow[svs[u] & 0x7fffffffu] : __ldg(row + (svs[u] & 0x7fffffffu));
+            if (!(svs[u] >> 31)) v[u] = -v[u];
+          }
         }
-        ot[e] = v;
+        __stcs(ot + 2 * q, make_double2(v[0], v[1]));
+        __stcs(ot + 2 * q + 1, make_double2(v[2], v[3]));
       }
     }
     __syncthreads();
@@ -253,6 +262,7 @@ void launch_materialize(const SlabPlan& P, const double* dAT, const double* dB, 
   const int64_t nmax = P.n_a > P.n_b ? P.n_a : P.n_b;
   const size_t smem = (size_t)nmax * 8;
   const int64_t SA = P.slots_a(), SB = P.slots_b();
+  if (SA % 4 || SB % 4) throw runtime_error("materialize: segment slots must be a multiple of 4");
   ProfScope prof("materialize", s);
   count_launch();
   if (smem <= 200 * 1024) {

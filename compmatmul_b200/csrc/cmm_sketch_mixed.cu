@@ -599,13 +599,16 @@ void launch_row_scale_f32(const float* dAT, const float* dB, int64_t n_a, int64_
 }
 
 // materialize fp32 rows (same slot layout as the FP64 path)
-__global__ void __launch_bounds__(512) k_materialize_f32(const float* __restrict__ AT,
-                                                        const float* __restrict__ B, int64_t n_a,
-                                                        int64_t n_b, int64_t k0, int d,
-                                                        const uint32_t* __restrict__ srcA,
-                                                        const uint32_t* __restrict__ srcB, int64_t SA,
-                                                        int64_t SB, int64_t kc, float* __restrict__ outA,
-                                                        float* __restrict__ outB, int stage) {
+// FP32 copies of the rows in slot order, as k_materialize: 1024 threads
+// per inner index, four consecutive slots per thread (one 16-byte index
+// load, one 16-byte streaming store)
+__global__ void __launch_bounds__(1024) k_materialize_f32(const float* __restrict__ AT,
+                                                         const float* __restrict__ B, int64_t n_a,
+                                                         int64_t n_b, int64_t k0, int d,
+                                                         const uint32_t* __restrict__ srcA,
+                                                         const uint32_t* __restrict__ srcB, int64_t SA,
+                                                         int64_t SB, int64_t kc, float* __restrict__ outA,
+                                                         float* __restrict__ outB, int stage) {
   extern __shared__ float srowf[];
   const int64_t kk = blockIdx.x;
   for (int side = 0; side < 2; ++side) {
@@ -619,16 +622,21 @@ __global__ void __launch_bounds__(512) k_materialize_f32(const float* __restrict
       __syncthreads();
     }
     for (int t = 0; t < d; ++t) {
-      const uint32_t* st = src + (size_t)t * S;
-      float* ot = out + ((size_t)t * kc + kk) * S;
-      for (int64_t e = threadIdx.x; e < S; e += blockDim.x) {
-        const uint32_t sv = __ldg(st + e);
-        float v = 0.f;
-        if (sv != kPadSlot) {
-          v = stage ? srowf[sv & 0x7fffffffu] : __ldg(row + (sv & 0x7fffffffu));
-          if (!(sv >> 31)) v = -v;
+      const uint4* st = reinterpret_cast<const uint4*>(src + (size_t)t * S);
+      float4* ot = reinterpret_cast<float4*>(out + ((size_t)t * kc + kk) * S);
+      for (int64_t q = threadIdx.x; q < S / 4; q += blockDim.x) {
+        const uint4 sv = __ldg(st + q);
+        const uint32_t svs[4] = {sv.x, sv.y, sv.z, sv.w};
+        float v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          v[u] = 0.f;
+          if (svs[u] != kPadSlot) {
+            v[u] = stage ? srowf[svs[u] & 0x7fffffffu] : __ldg(row + (svs[u] & 0x7fffffffu));
+            if (!(svs[u] >> 31)) v[u] = -v[u];
+          }
         }
-        ot[e] = v;
+        __stcs(ot + q, make_float4(v[0], v[1], v[2], v[3]));
       }
     }
     __syncthreads();
@@ -642,11 +650,12 @@ void launch_materialize_f32(const SlabPlan& P, const float* dAT, const float* dB
   const size_t smem = (size_t)nmax * 4;
   const int stage = smem <= 200 * 1024 ? 1 : 0;
   const int64_t SA = P.slots_a(), SB = P.slots_b();
+  if (SA % 4 || SB % 4) throw runtime_error("materialize: segment slots must be a multiple of 4");
   ProfScope prof("materialize", s);
   count_launch();
   if (stage)
     CMM_CUDA(cudaFuncSetAttribute(k_materialize_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_materialize_f32<<<(unsigned)kc, 512, stage ? smem : 0, s>>>(dAT, dB, P.n_a, P.n_b, k0, P.d,
+  k_materialize_f32<<<(unsigned)kc, 1024, stage ? smem : 0, s>>>(dAT, dB, P.n_a, P.n_b, k0, P.d,
                                                                 P.srcA.as<uint32_t>(), P.srcB.as<uint32_t>(),
                                                                 SA, SB, kc, dOutA, dOutB, stage);
   CMM_CUDA(cudaGetLastError());
