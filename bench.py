@@ -635,13 +635,16 @@ def leg_mixed_vs_fp64(workload, variant, warm=2, steps=3, warm64=1, steps64=2):
     i64 = torch.as_tensor(top64[0].astype(np.int64), device=C32.device)
     j64 = torch.as_tensor(top64[1].astype(np.int64), device=C32.device)
     got = C32[i64, j64].cpu().numpy()
-    rel = np.abs(got - top64[2]) / np.maximum(np.abs(top64[2]), 1e-300)
+    want = C64[i64, j64].cpu().numpy()
+    rel = np.abs(got - want) / np.maximum(np.abs(want), 1e-300)
+    dense_diff = float((C32 - C64).abs().max())
     mixed.update({"fp64_same_inputs": {"ms_per_step": fp64["ms_per_step"], "clocks": fp64["clocks"],
                                        "recovered_planted": fp64["recovered_planted"]},
                   "speedup_vs_fp64": fp64["ms_per_step"] / mixed["ms_per_step"],
                   "same_set_as_fp64": set(zip(top32[0].tolist(), top32[1].tolist()))
                   == set(zip(top64[0].tolist(), top64[1].tolist())),
-                  "max_rel_err_recovered_vs_fp64": float(rel.max())})
+                  "max_rel_err_recovered_vs_fp64": float(rel.max()),
+                  "max_abs_diff_dense_vs_fp64": dense_diff})
     del C32, C64
     torch.cuda.empty_cache()
     return mixed
