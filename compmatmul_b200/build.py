@@ -29,7 +29,7 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
 
 CUDA_SOURCES = ["cmm_sketch.cu", "cmm_sketch_v1.cu", "cmm_sketch_mixed.cu", "cmm_sketch_cluster.cu",
                 "cmm_plan.cu", "cmm_recover.cu", "cmm_noalloc.cu", "cmm_probe.cu", "cmm_batch.cu", "cmm_serve.cu"]
-HOST_SOURCES = ["cmm_hashparams.cpp", "cmm_capi.cpp"]
+HOST_SOURCES = ["cmm_hashparams.cpp", "cmm_capi.cpp", "cmm_hostcopy.cpp"]
 
 
 def _run(cmd, verbose=False):

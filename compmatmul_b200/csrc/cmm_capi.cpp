@@ -188,8 +188,8 @@ static cudaStream_t copy_stream() {
 // matrices and hand a feed to the sketch; its chunk loop calls wait() before
 // the first use of rows [k0, k0 + c).  The copies run on copy_stream() in
 // pieces of the sketch's chunk size, one event each, issued one piece ahead
-// of the chunk being computed (so pageable host memory, whose copies block
-// the host, still overlaps the previous chunk's kernels).
+// of the chunk being computed (pageable host memory is staged by host
+// threads, host_to_device, while the previous chunk's kernels run).
 class RowFeed {
  public:
   RowFeed(const void* hAT, const void* hB, void* dAT, void* dB, int64_t n_a, int64_t n_b,
@@ -235,8 +235,8 @@ class RowFeed {
   };
   void issue() {
     const int64_t k0 = issued_, c = n_inner_ - k0 < piece_ ? n_inner_ - k0 : piece_;
-    if (rowA_) CMM_CUDA(cudaMemcpyAsync(dAT_ + k0 * rowA_, hAT_ + k0 * rowA_, c * rowA_, cudaMemcpyHostToDevice, cs_));
-    if (rowB_) CMM_CUDA(cudaMemcpyAsync(dB_ + k0 * rowB_, hB_ + k0 * rowB_, c * rowB_, cudaMemcpyHostToDevice, cs_));
+    if (rowA_) host_to_device(dAT_ + k0 * rowA_, hAT_ + k0 * rowA_, c * rowA_, cs_);
+    if (rowB_) host_to_device(dB_ + k0 * rowB_, hB_ + k0 * rowB_, c * rowB_, cs_);
     Piece pc{k0, nullptr, false};
     CMM_CUDA(cudaEventCreateWithFlags(&pc.ev, cudaEventDisableTiming));
     CMM_CUDA(cudaEventRecord(pc.ev, cs_));
@@ -468,8 +468,9 @@ static uint64_t pick_seed(int has_seed, uint64_t seed) { return has_seed ? seed 
 // The dense estimate comes back to the host in row blocks: every block's
 // decompression is enqueued on s first, then each block's copy on
 // copy_stream() after its event, so the copies overlap the decompression of
-// the later blocks (with pageable host memory too, whose copies block the
-// host).  Returns when C is on the host.
+// the later blocks (pageable host memory: each block is drained through the
+// staging slots, device_to_host, while later blocks decompress).  Returns
+// when C is on the host.
 static void decompress_to_host(int variant, int d, int b, int64_t n_a, int64_t n_b, const Codes& codes,
                                const double* dP, double* dC, double* C, cudaStream_t s) {
   struct Join {  // s waits for the copies before anything later (frees) runs on it
@@ -501,7 +502,7 @@ static void decompress_to_host(int variant, int d, int b, int64_t n_a, int64_t n
     for (int64_t i0 = 0; i0 < n_a; i0 += rows, ++blk) {
       const int64_t r = n_a - i0 < rows ? n_a - i0 : rows;
       CMM_CUDA(cudaStreamWaitEvent(join.cs, join.ev[blk], 0));
-      CMM_CUDA(cudaMemcpyAsync(C + i0 * n_b, dC + i0 * n_b, (size_t)r * n_b * 8, cudaMemcpyDeviceToHost, join.cs));
+      device_to_host(C + i0 * n_b, dC + i0 * n_b, (size_t)r * n_b * 8, join.cs);
     }
   }
   CMM_CUDA(cudaStreamSynchronize(join.cs));

@@ -67,6 +67,15 @@ struct SketchParams {
 };
 SketchParams make_sketch_params(int kind, int d, int b, uint64_t seed);
 
+// ------------------------------------------------------ host copies
+// Copies between device memory and caller-owned host memory (cmm_hostcopy.cpp).
+// Pinned host memory: cudaMemcpyAsync on cs.  Pageable host memory: through
+// pinned staging slots filled / drained by several host threads;
+// host_to_device returns once the source has been read, device_to_host once
+// dst holds the data (pinned: enqueued only).
+void host_to_device(void* dst, const void* src, size_t bytes, cudaStream_t cs);
+void device_to_host(void* dst, const void* src, size_t bytes, cudaStream_t cs);
+
 // ---------------------------------------------------------- device pool
 // Stream-ordered scratch allocation (cudaMallocAsync) with RAII release.
 struct DevBuf {
