@@ -529,8 +529,9 @@ def run_serve(args, rank, extra, compare_fp64):
                 "clocks": clk}
 
     main_run = run(pool, True, arrivals)
-    # steady state: every request left within the arrival window plus one p99
-    main_run["kept_up"] = bool(main_run["span_s"] <= secs + 1.0 + main_run["p99_ms"] / 1e3)
+    # steady state: the server completed requests as fast as they arrived
+    # (over the whole run, drain included)
+    main_run["kept_up"] = bool(main_run["products_per_s"] >= 0.97 * main_run["offered_per_s"])
     out = {"value": main_run["products_per_s"], "steps": main_run["requests"], "warmup": len(pool),
            "ms_per_step": 1e3 / main_run["products_per_s"],
            "latency_ms": {"p50": main_run["p50_ms"], "p99": main_run["p99_ms"], "mean": main_run["mean_ms"]},
