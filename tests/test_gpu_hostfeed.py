@@ -79,3 +79,28 @@ def test_dense_estimate_row_blocks(gpu, variant, d, n_a):
     C_host = capi.matmul(variant, None, AT, B, d, 1 << 16, 5)
     C_dev = device.matmul(torch.from_numpy(AT).cuda(), torch.from_numpy(B).cuda(), d, 1 << 16, 5, variant)
     assert np.array_equal(C_host, C_dev.cpu().numpy())
+
+
+@pytest.mark.parametrize("variant", ["fft", "fwht"])
+def test_pinned_and_pageable_host_buffers_agree(gpu, variant):
+    """The host entry point copies page-locked buffers directly and pageable
+    ones through its pinned staging slots (several host threads): the same
+    chunks, so the same sketch and dense estimate bit for bit.  The product
+    is larger than one 64 MB staging slot per matrix, so several slots are
+    in flight."""
+    import ctypes as C
+
+    import torch
+
+    from compmatmul_b200 import HASH_KINDS, VARIANTS, capi, lib
+    rng = np.random.default_rng(23)
+    AT = rng.standard_normal((2100, 4096))
+    B = rng.standard_normal((2100, 4000))
+    d, b, seed = 3, 1 << 15, 5
+    C_page = capi.matmul(variant, None, AT, B, d, b, seed)
+    hAT, hB = torch.from_numpy(AT).pin_memory(), torch.from_numpy(B).pin_memory()
+    hC = torch.empty((4096, 4000), dtype=torch.float64).pin_memory()
+    rc = lib().cmm_matmul(VARIANTS[variant], HASH_KINDS[None], 4096, 2100, 4000, C.c_void_p(hC.data_ptr()),
+                          C.c_void_p(hAT.data_ptr()), C.c_void_p(hB.data_ptr()), d, b, 1, seed)
+    assert rc == 0, lib().cmm_last_error()
+    assert np.array_equal(C_page, hC.numpy())
