@@ -12,9 +12,10 @@ d = 9, FFT variant, K = 256 (inputs 4.3 GB > L2, so no flush is needed).
 
 The default single-GPU run also measures the other workloads as short legs,
 reported as extra keys of the same JSON line ("legs"): config 2 FWHT at
-n = 16384, config 2 at n = 4096 (both variants), config 3 (mixed precision,
-FFT and FWHT, against the FP64 path on the same inputs), config 4 (256
-uneven products in one batch plan) and a bounded config 5 serving run.
+n = 16384, config 1 (n = 512, FFT), config 2 at n = 4096 (both variants),
+config 3 (mixed precision, FFT and FWHT, against the FP64 path on the same
+inputs), config 4 (256 uneven products in one batch plan) and a bounded
+config 5 serving run.
 Each leg states its steps, its clocks and its result check.
 
 --gpus N > 1 runs under torchrun, one rank per GPU, each rank an
@@ -674,6 +675,14 @@ def run_legs(args, reps, dAT, dB, dC, L):
         guard(f"config2_n16384_{other}",
               lambda: leg_product("config2_n16384", dAT, dB, w["d"], w["b"], w["seed"], other, w["K"], 3, 5,
                                   golden=golden_sets("config2_n16384", other), out=dC)[0])
+    w1 = WORKLOADS["config1"]
+
+    def config1():
+        AT, B, pl = planted_problem(w1["n"], w1["n"], w1["n"], w1["K"], w1["gen_seed"])
+        A_d, B_d = torch.from_numpy(AT).cuda(), torch.from_numpy(B).cuda()
+        return leg_product("config1", A_d, B_d, w1["d"], w1["b"], w1["seed"], "fft", w1["K"], 3, 20,
+                           golden=golden_sets("config1", "fft"), planted=pl)[0]
+    guard("config1", config1)
     w4 = WORKLOADS["config2_n4096"]
 
     def n4096():
