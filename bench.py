@@ -791,6 +791,9 @@ def main():
 
     barrier = reps.barrier
     clocks = ClockSampler(torch.cuda.current_device())
+    import ctypes as C
+    phase_cyc, phase_steps = (C.c_double * 6)(), C.c_double(0.0)
+    phases_on = L.cmm_cluster_phase_cycles(phase_cyc, C.byref(phase_steps)) == 0  # clears (instrumented builds)
     L.cmm_profile_reset()
     L.cmm_profile_enable(1)
     launches0 = L.cmm_launch_count()
@@ -810,6 +813,12 @@ def main():
     fam = {f: cmb.profile_read(f) for f in ("hash", "scale", "plan", "materialize", "sketch",
                                              "finalize", "decompress", "topk")}
     sketch_kernel = L.cmm_last_sketch_kernel().decode()
+    phases = None
+    if phases_on and L.cmm_cluster_phase_cycles(phase_cyc, C.byref(phase_steps)) == 0 and phase_steps.value:
+        names = ["clear", "wait_staged_row", "scatter", "radix_passes", "cluster_barrier", "combine"]
+        phases = {"cycles_per_cta_step": {nm: phase_cyc[i] / phase_steps.value for i, nm in enumerate(names)},
+                  "cta_steps": phase_steps.value,
+                  "note": "thread 0 of each CTA, clock64 between phase marks; instrumented build (CMM_PHASE_CLOCKS)"}
     value = reps.throughput(args.steps, total_ms / 1e3)  # products of all ranks / slowest rank
     total_ms = reps.max(total_ms)
     ms_per_step = total_ms / args.steps
@@ -937,6 +946,8 @@ def main():
     }
     if fp64_ms is not None:
         line["plain_fp64_same_inputs"] = {"ms_per_step": fp64_ms, "speedup": fp64_ms / ms_per_step}
+    if phases is not None:
+        line["cluster_phase_cycles"] = phases
     if legs is not None:
         line["legs"] = legs
     print(json.dumps(line), flush=True)

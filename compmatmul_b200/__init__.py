@@ -40,6 +40,7 @@ EXPORTED = [
     "cmm_batch_info", "cmm_batch_config", "cmm_batch_destroy", "cmm_server_create", "cmm_server_submit",
     "cmm_server_wait", "cmm_server_stats_get", "cmm_server_destroy", "cmm_dev_decompress_entries",
     "cmm_dev_sketch_topk", "cmm_rng_seed", "cmm_rng_next", "cmm_time_millis", "cmm_hash_params",
+    "cmm_cluster_phase_cycles",
 ]
 
 
@@ -110,6 +111,7 @@ def lib():
     L.cmm_rng_next.restype = u64
     L.cmm_time_millis.restype = u64
     L.cmm_hash_params.argtypes = [i32, i32, u64, u64, vp, _C.c_size_t]
+    L.cmm_cluster_phase_cycles.argtypes = [_C.POINTER(_C.c_double), _C.POINTER(_C.c_double)]
     for name in EXPORTED:
         if name not in ("cmm_last_error", "cmm_version", "cmm_profile_enable", "cmm_last_sketch_kernel",
                         "cmm_profile_reset", "cmm_launch_count", "cmm_rng_seed", "cmm_rng_next",

@@ -26,6 +26,9 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                   "--expt-relaxed-constexpr", "-I" + INCLUDE, "-I" + CSRC]
+# extra flags for instrumented builds, e.g. CMM_EXTRA_NVFLAGS=-DCMM_PHASE_CLOCKS
+# (per-phase cycle counts of the cluster sketch kernel)
+NVFLAGS += os.environ.get("CMM_EXTRA_NVFLAGS", "").split()
 
 CUDA_SOURCES = ["cmm_sketch.cu", "cmm_sketch_v1.cu", "cmm_sketch_mixed.cu", "cmm_sketch_cluster.cu",
                 "cmm_plan.cu", "cmm_recover.cu", "cmm_noalloc.cu", "cmm_probe.cu", "cmm_batch.cu", "cmm_serve.cu"]

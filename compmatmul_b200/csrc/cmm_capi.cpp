@@ -694,6 +694,13 @@ int cmm_server_destroy(void* server) {
   return guarded([&] { server_destroy(static_cast<Server*>(server)); });
 }
 
+int cmm_cluster_phase_cycles(double* cycles, double* steps) {
+  return guarded([&] {
+    if (!cluster_phase_cycles(cycles, steps))
+      throw unsupported("built without CMM_PHASE_CLOCKS (set CMM_EXTRA_NVFLAGS=-DCMM_PHASE_CLOCKS and rebuild)");
+  });
+}
+
 int cmm_probe_fma_tflops(int fp64, double* tflops) {
   return guarded([&] {
     if (!tflops) throw invalid_argument("tflops must not be null");

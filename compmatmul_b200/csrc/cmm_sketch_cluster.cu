@@ -119,6 +119,31 @@ __device__ __forceinline__ void h16(float* buf, const uint32_t (&hb)[2][2], int 
 
 }  // namespace
 
+// Per-phase cycle counts of the cluster kernel, compiled in only with
+// -DCMM_PHASE_CLOCKS (python -m compmatmul_b200.build with
+// CMM_EXTRA_NVFLAGS=-DCMM_PHASE_CLOCKS): thread 0 of every CTA adds the
+// clock64() time of each phase of each inner index to g_cl_phase, which
+// cmm_cluster_phase_cycles() reads and clears.  Phases: 0 clear the
+// buffer, 1 wait for the staged row (cp.async + barrier), 2 scatter, 3 the
+// local radix passes, 4 the cluster barrier before the combine, 5 the
+// combine and accumulation (with its barrier when single-buffered).
+constexpr int kClPhases = 6;
+#ifdef CMM_PHASE_CLOCKS
+__device__ unsigned long long g_cl_phase[kClPhases + 1];  // + inner indices timed
+#define CL_MARK(ph)                                                        \
+  do {                                                                     \
+    if (tid == 0) {                                                        \
+      const long long now_ = clock64();                                    \
+      if ((ph) >= 0) atomicAdd(&g_cl_phase[(ph)], (unsigned long long)(now_ - t_ph)); \
+      t_ph = now_;                                                         \
+    }                                                                      \
+  } while (0)
+#else
+#define CL_MARK(ph) \
+  do {              \
+  } while (0)
+#endif
+
 struct ClArgs {
   const void* matA;  // [t][kk][R2][SA]
   const void* matB;
@@ -384,7 +409,11 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
   if (kk < ke) stage(kk);
   cluster.sync();  // tables and codes written; the previous item's reads are done
 
+#ifdef CMM_PHASE_CLOCKS
+  long long t_ph = 0;
+#endif
   while (kk < ke) {
+    CL_MARK(-1);
     const int64_t kn = next_k(kk + 1);
     Real alpha = (Real)1, beta = (Real)1;
     if (kFFT) {
@@ -400,8 +429,10 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
     } else {
       for (int e = tid; e < PL; e += kCT) { xs[e] = (Real)0; ys[e] = (Real)0; }
     }
+    CL_MARK(0);
     cp_async_wait_all();  // this thread's copies of row kk; the barrier publishes all
     __syncthreads();
+    CL_MARK(1);
     // ---- scatter this CTA's residue segment.  The plan cuts the segment at
     // bucket boundaries, so every bucket has one writer thread; its slots are
     // sorted by bucket.  Per batch of kCBatch slots a thread loads every
@@ -479,6 +510,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
       if (side == 0 && !split) __syncthreads();
     }
     __syncthreads();         // the scatter is done with the staged row
+    CL_MARK(2);
     if (kn < ke) stage(kn);  // overlaps the transform and the combine
 
     // ---- local transform of length L (results stay in shared memory)
@@ -625,7 +657,9 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
       }
     }
 
+    CL_MARK(3);
     cluster.sync();  // every sub-spectrum of the cluster is complete
+    CL_MARK(4);
 
     // ---- radix-R2 combine across the cluster; accumulate.  With R2 = 16 the
     // two threads of a lane pair own the even / odd outputs of one position:
@@ -700,6 +734,10 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
       }
     }
     if (NB == 1) cluster.sync();  // all reads of the sub-spectra are done
+    CL_MARK(5);
+#ifdef CMM_PHASE_CLOCKS
+    if (tid == 0) atomicAdd(&g_cl_phase[kClPhases], 1ull);
+#endif
     ++step;
     kk = kn;
   }
@@ -718,6 +756,26 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
 }
 
 // ------------------------------------------------------------------ host
+// Sums of the per-phase cycles over all CTAs and inner indices since the
+// last call, and the number of (CTA, inner index) steps timed; false when
+// the library was built without CMM_PHASE_CLOCKS.
+bool cluster_phase_cycles(double* cycles, double* steps) {
+#ifdef CMM_PHASE_CLOCKS
+  unsigned long long h[kClPhases + 1];
+  CMM_CUDA(cudaDeviceSynchronize());
+  CMM_CUDA(cudaMemcpyFromSymbol(h, g_cl_phase, sizeof(h)));
+  const unsigned long long zero[kClPhases + 1] = {};
+  CMM_CUDA(cudaMemcpyToSymbol(g_cl_phase, zero, sizeof(zero)));
+  for (int i = 0; i < kClPhases; ++i) cycles[i] = (double)h[i];
+  *steps = (double)h[kClPhases];
+  return true;
+#else
+  for (int i = 0; i < kClPhases; ++i) cycles[i] = 0.0;
+  *steps = 0.0;
+  return false;
+#endif
+}
+
 static int cl_logL(int variant, bool f32) { return (variant == kVariantFFT && !f32) ? 12 : 13; }
 
 bool sketch_cluster_applicable(int variant, bool f32, int b) {

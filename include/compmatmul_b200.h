@@ -344,6 +344,13 @@ const char* cmm_last_sketch_kernel(void);
  * FMA; FP64 if fp64 != 0, else FP32), from a register-resident FMA loop
  * timed with CUDA events: the arithmetic roofline's denominator. */
 int cmm_probe_fma_tflops(int fp64, double* tflops);
+/* Per-phase cycles of the cluster sketch kernel, summed over its CTAs and
+ * inner indices since the last call (then cleared): cycles[0..5] = clearing
+ * the sub-spectrum buffer, waiting for the staged row, the scatter, the
+ * local radix passes, the cluster barrier, the combine + accumulation;
+ * *steps = (CTA, inner index) pairs timed.  Only in a library built with
+ * -DCMM_PHASE_CLOCKS (CMM_EXTRA_NVFLAGS); otherwise CMM_ERR_UNSUPPORTED. */
+int cmm_cluster_phase_cycles(double* cycles, double* steps);
 
 #ifdef __cplusplus
 }
