@@ -815,7 +815,7 @@ def main():
     sketch_kernel = L.cmm_last_sketch_kernel().decode()
     phases = None
     if phases_on and L.cmm_cluster_phase_cycles(phase_cyc, C.byref(phase_steps)) == 0 and phase_steps.value:
-        names = ["clear", "wait_staged_row", "scatter", "radix_passes", "cluster_barrier", "combine"]
+        names = ["radix_passes", "wait_staged_row", "scatter", "group_barrier_wait", "combine", "unused"]
         phases = {"cycles_per_cta_step": {nm: phase_cyc[i] / phase_steps.value for i, nm in enumerate(names)},
                   "cta_steps": phase_steps.value,
                   "note": "thread 0 of each CTA, clock64 between phase marks; instrumented build (CMM_PHASE_CLOCKS)"}

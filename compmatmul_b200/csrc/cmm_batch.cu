@@ -447,15 +447,24 @@ __global__ void __launch_bounds__(kBT, 1)
         for (int j = 0; j < 4; ++j) {
           const int m = tid + j * kBT;
           if (m < L) {
+            if constexpr (kF32) {
+              // the two rows' Z^2 are summed in FP32 (one rounding, like
+              // each row's own), then added to the compensated pair
+              C* zp0 = bufA(0) + ph<EC>(m);
+              C* zp1 = bufA(1) + ph<EC>(m);
+              const C z0 = *zp0, z1 = *zp1;
+              *zp0 = mk((Real)0, (Real)0);  // clear for the next rows
+              *zp1 = mk((Real)0, (Real)0);
+              const float re = fmaf(-z1.y, z1.y, fmaf(z1.x, z1.x, fmaf(-z0.y, z0.y, z0.x * z0.x)));
+              const float im = fmaf(z1.x, z1.y, z0.x * z0.y);
+              tsum(acc[2 * j], lo[2 * j], re);
+              tsum(acc[2 * j + 1], lo[2 * j + 1], im + im);
+            } else {
 #pragma unroll
-            for (int qq = 0; qq < KB; ++qq) {
-              C* zp = bufA(qq) + ph<EC>(m);
-              const C z = *zp;
-              *zp = mk((Real)0, (Real)0);  // clear for the next row
-              if constexpr (kF32) {
-                tsum(acc[2 * j], lo[2 * j], z.x * z.x - z.y * z.y);
-                tsum(acc[2 * j + 1], lo[2 * j + 1], (z.x + z.x) * z.y);
-              } else {
+              for (int qq = 0; qq < KB; ++qq) {
+                C* zp = bufA(qq) + ph<EC>(m);
+                const C z = *zp;
+                *zp = mk((Real)0, (Real)0);  // clear for the next row
                 acc[2 * j] = fma(z.x, z.x, fma(-z.y, z.y, acc[2 * j]));
                 acc[2 * j + 1] = fma(z.x + z.x, z.y, acc[2 * j + 1]);
               }
@@ -467,15 +476,27 @@ __global__ void __launch_bounds__(kBT, 1)
         for (int j = 0; j < 8; ++j) {
           const int m = tid + j * kBT;
           if (m < L) {
+            if constexpr (kF32) {  // the two rows summed in FP32 first, as for the FFT
+              Real* xp0 = xsq(0) + ph<ER>(m);
+              Real* yp0 = ysq(0) + ph<ER>(m);
+              Real* xp1 = xsq(1) + ph<ER>(m);
+              Real* yp1 = ysq(1) + ph<ER>(m);
+              const float sxy = fmaf(*xp1, *yp1, *xp0 * *yp0);
+              *xp0 = 0.f;  // clear for the next rows
+              *yp0 = 0.f;
+              *xp1 = 0.f;
+              *yp1 = 0.f;
+              tsum(acc[j], lo[j], sxy);
+            } else {
 #pragma unroll
-            for (int qq = 0; qq < KB; ++qq) {
-              Real* xp = xsq(qq) + ph<ER>(m);
-              Real* yp = ysq(qq) + ph<ER>(m);
-              const Real xv = *xp, yv = *yp;
-              *xp = (Real)0;  // clear for the next row
-              *yp = (Real)0;
-              if constexpr (kF32) tsum(acc[j], lo[j], xv * yv);
-              else acc[j] = fma(xv, yv, acc[j]);
+              for (int qq = 0; qq < KB; ++qq) {
+                Real* xp = xsq(qq) + ph<ER>(m);
+                Real* yp = ysq(qq) + ph<ER>(m);
+                const Real xv = *xp, yv = *yp;
+                *xp = (Real)0;  // clear for the next row
+                *yp = (Real)0;
+                acc[j] = fma(xv, yv, acc[j]);
+              }
             }
           }
         }

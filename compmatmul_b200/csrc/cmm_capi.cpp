@@ -471,6 +471,12 @@ static uint64_t pick_seed(int has_seed, uint64_t seed) { return has_seed ? seed 
 // the later blocks (pageable host memory: each block is drained through the
 // staging slots, device_to_host, while later blocks decompress).  Returns
 // when C is on the host.
+// a synchronous entry point reports a group barrier wait that ran out
+static void check_group_waits() {
+  if (sketch_group_timed_out())
+    throw std::runtime_error("cluster sketch: a group barrier wait ran out; the sketch is invalid");
+}
+
 static void decompress_to_host(int variant, int d, int b, int64_t n_a, int64_t n_b, const Codes& codes,
                                const double* dP, double* dC, double* C, cudaStream_t s) {
   struct Join {  // s waits for the copies before anything later (frees) runs on it
@@ -507,6 +513,7 @@ static void decompress_to_host(int variant, int d, int b, int64_t n_a, int64_t n
   }
   CMM_CUDA(cudaStreamSynchronize(join.cs));
   CMM_CUDA(cudaStreamSynchronize(s));
+  check_group_waits();
 }
 
 // ------------------------------------------------------- instrumentation
@@ -952,6 +959,7 @@ int cmm_compressed_product_f32(int variant, int hash_kind, int64_t n_a, int64_t 
                         P.as<double>(), s, &feed);
     CMM_CUDA(cudaMemcpyAsync(p_out, P.ptr, P.bytes, cudaMemcpyDeviceToHost, s));
     CMM_CUDA(cudaStreamSynchronize(s));
+    check_group_waits();
   });
 }
 
@@ -993,6 +1001,7 @@ int cmm_compressed_product(int variant, int hash_kind, int64_t n_a, int64_t n_in
                   P.as<double>(), s, &feed);
     CMM_CUDA(cudaMemcpyAsync(p_out, P.ptr, P.bytes, cudaMemcpyDeviceToHost, s));
     CMM_CUDA(cudaStreamSynchronize(s));
+    check_group_waits();
   });
 }
 

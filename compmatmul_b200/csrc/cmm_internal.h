@@ -226,6 +226,9 @@ void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const Sl
                            const void* dMatA, const void* dMatB, int64_t kc, const int* dScaleExp,
                            int64_t k0, const double2* dTw, void* dPartial, int d, int accumulate,
                            cudaStream_t s);
+// true (and cleared) when a group barrier wait of a cluster-kernel launch
+// ran out since the last call; that launch wrote NaN partials
+bool sketch_group_timed_out();
 // per-phase cycle sums of the cluster kernel (CMM_PHASE_CLOCKS builds only)
 bool cluster_phase_cycles(double* cycles6, double* steps);
 // finalize for partials in natural frequency order (cluster kernels)

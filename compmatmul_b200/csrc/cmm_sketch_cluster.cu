@@ -5,36 +5,40 @@
 //    interleaved slabs (f = R1 f' + r1 for the FFT; f = r1 (b / R1) + f' for
 //    the FWHT); each slab is a length M = b / R1 transform of
 //      u_r1[n1] = tw(n1, r1) * sum_q1 w(q1, r1) x[q1 M + n1];
-//  * a thread-block cluster of R2 CTAs computes one slab by decimation in
-//    time: CTA r2 takes the members of residue class n1 mod R2 only (the
-//    bucket-sorted plan hands each CTA its own segment of every row, so an
-//    index is scattered by R1 CTAs instead of by every slab), sums them into
-//    its length-L sub-sequence and transforms it in shared memory;
+//  * a group of R2 CTAs computes one slab by decimation in time: CTA r2
+//    takes the members of residue class n1 mod R2 only (the bucket-sorted
+//    plan hands each CTA its own segment of every row, so an index is
+//    scattered by R1 CTAs instead of by every slab), sums them into its
+//    length-L sub-sequence and transforms it in shared memory;
 //  * the R2 sub-spectra are combined by a radix-R2 DFT/WHT across the
-//    cluster, reading the other CTAs' shared memory (DSMEM): CTA r2 owns the
-//    frequencies of L / R2 sub-spectrum positions and accumulates
+//    group: the last radix pass writes each CTA's sub-spectrum to an
+//    exchange area in global memory, which stays in L2 (R2 x L elements per
+//    group, double-buffered), and after the group barrier CTA r2 reads the
+//    R2 values of its L / R2 sub-spectrum positions back and accumulates
 //    Z^2 (FFT, z = alpha x + i beta y) or X * Y (FWHT) for them over k.
-//  With two sub-spectrum buffers (when they fit in shared memory) one
-//  cluster barrier per inner index both publishes the new sub-spectra and
-//  retires the reads of the buffer written next; with one buffer a second
-//  barrier follows the combine.  Every CTA of a cluster runs the same k
-//  sequence (all-zero rows are skipped by all of them), so all of them
-//  reach every barrier.
-//  The next row's segments are staged with cp.async while the current one
-//  is transformed and combined.
+//    Thread-block clusters exchanging through distributed shared memory were
+//    the earlier form: clusters of 8 fit 15 times on the 148 SMs, and the
+//    remote reads ran at about a third of their port's peak.
+//  The grid is one cooperative launch of every resident CTA, in groups of
+//  R2; a group barrier is a counter in global memory.  It is split (arrive
+//  after the exchange write, wait before the combine) and the next row's
+//  scatter runs in between; the row after that is staged with cp.async
+//  while the current one is combined and transformed.  Every CTA of a group
+//  runs the same k sequence (all-zero rows are skipped by all of them), so
+//  all of them reach every barrier.
 // Instantiations: FFT/FWHT x FP64/FP32 (FP32 = mixed precision: FP32 data,
 // two-sum compensated accumulation, tensor-core Hadamard-16 stages for the
-// FWHT, FP64 partials) x one or two buffers.
-#include <cooperative_groups.h>
+// FWHT, FP64 partials).
 #include <cuda_bf16.h>
 
 #include <cstdio>
+#include <mutex>
+#include <stdexcept>
 #include <cstdlib>
 
 #include "cmm_fft_device.cuh"
 #include "cmm_internal.h"
 
-namespace cg = cooperative_groups;
 
 namespace cmm {
 namespace {
@@ -123,10 +127,10 @@ __device__ __forceinline__ void h16(float* buf, const uint32_t (&hb)[2][2], int 
 // -DCMM_PHASE_CLOCKS (python -m compmatmul_b200.build with
 // CMM_EXTRA_NVFLAGS=-DCMM_PHASE_CLOCKS): thread 0 of every CTA adds the
 // clock64() time of each phase of each inner index to g_cl_phase, which
-// cmm_cluster_phase_cycles() reads and clears.  Phases: 0 clear the
-// buffer, 1 wait for the staged row (cp.async + barrier), 2 scatter, 3 the
-// local radix passes, 4 the cluster barrier before the combine, 5 the
-// combine and accumulation (with its barrier when single-buffered).
+// cmm_cluster_phase_cycles() reads and clears.  Phases: 0 the local radix
+// passes with the write of the sub-spectrum and the arrival, 1 wait for the
+// next staged row (cp.async + barrier), 2 its scatter, 3 the rest of the
+// group barrier (wait), 4 the combine and accumulation; 5 is unused.
 constexpr int kClPhases = 6;
 #ifdef CMM_PHASE_CLOCKS
 __device__ unsigned long long g_cl_phase[kClPhases + 1];  // + inner indices timed
@@ -154,6 +158,10 @@ struct ClArgs {
   const int* scale_exp;
   const double2* tw;  // w_b^j
   void* partial;      // [g][t][b] double2 (FFT) / double (FWHT)
+  void* xch;          // exchange area: [group][2][R2][L] complex (FFT) / (x, y) pairs (FWHT)
+  unsigned* gsync;    // arrival counters, one 128-byte line per group, zero at launch
+  int* timeout;       // host-mapped flag: a group wait ran out
+  unsigned spin_limit, wait_extra;
   int64_t SA, SB, kc, k0;
   int d, log2b, logR1, logR2, G, accumulate;
 };
@@ -173,14 +181,14 @@ __device__ __forceinline__ int64_t spad_len(int64_t n) { return spad_len_n(n, si
 __host__ __device__ inline int cl_pre_hi(int log2b) { return log2b > 9 ? 1 << (log2b - 9) : 1; }
 
 // Shared-memory layout of one CTA, shared by the kernel and the host sizing:
-// NB sub-spectrum buffers, then (FFT) the factored post-twiddle tables, the
+// the sub-spectrum buffer, then (FFT) the factored post-twiddle tables, the
 // DIF weight tables when R1 > 1, the pass twiddles and w_R1; then the staged
 // row values of this CTA's segments and their premixed codes.
 struct ClLayout {
   size_t buf, post, pre, ptw, wr, stage, codes, total;
 };
 __host__ __device__ inline size_t cl_align16(size_t x) { return (x + 15) & ~(size_t)15; }
-__host__ __device__ inline ClLayout cl_layout(bool fft, bool f32, bool u16, int NB, int R1, int log2b,
+__host__ __device__ inline ClLayout cl_layout(bool fft, bool f32, bool u16, int R1, int log2b,
                                               int64_t SA, int64_t SB) {
   const size_t real = f32 ? 4 : 8, cpx = 2 * real;
   const size_t L = (fft && !f32) ? 4096 : 8192;
@@ -188,7 +196,7 @@ __host__ __device__ inline ClLayout cl_layout(bool fft, bool f32, bool u16, int 
   ClLayout o;
   size_t p = 0;
   o.buf = p;
-  p += (size_t)NB * (fft ? plen(L, cpx) * cpx : 2 * plen(L, real) * real);
+  p += fft ? plen(L, cpx) * cpx : 2 * plen(L, real) * real;
   o.post = p;
   if (fft) p += (128 + 64) * cpx;
   o.pre = p;
@@ -217,10 +225,14 @@ static __device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc) {
 }
 static __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// VARIANT 0 = FFT, 1 = FWHT; Real = double (plain) or float (mixed); NB = 2
-// double-buffers the sub-spectra (one cluster barrier per inner index), NB = 1
-// when two buffers do not fit in shared memory (two barriers).
-template <int VARIANT, typename Real, typename CodeT, int NB>
+static __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// VARIANT 0 = FFT, 1 = FWHT; Real = double (plain) or float (mixed).
+template <int VARIANT, typename Real, typename CodeT>
 __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
   constexpr bool kFFT = VARIANT == kVariantFFT;
   constexpr bool kF32 = sizeof(Real) == 4;
@@ -232,17 +244,16 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
   constexpr int OUT = L / kCT;  // outputs per thread (8 or 16)
 
   extern __shared__ __align__(16) unsigned char sm[];
-  cg::cluster_group cluster = cg::this_cluster();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int R1 = 1 << a.logR1, R2 = 1 << a.logR2;
-  const int r2 = (int)cluster.block_rank();
+  const int r2 = (int)blockIdx.x;  // this CTA's residue class; blockIdx.y is its group
   const int logM = a.log2b - a.logR1;  // M = b / R1
   const double2* tw = a.tw;
 
   // ---- shared layout (cl_layout)
-  const ClLayout lay = cl_layout(kFFT, kF32, sizeof(CodeT) == 2, NB, R1, a.log2b, a.SA, a.SB);
-  C* buf0 = reinterpret_cast<C*>(sm + lay.buf);        // FFT: NB x PL complex
-  Real* xs0 = reinterpret_cast<Real*>(sm + lay.buf);   // FWHT: NB x (x: PL, y: PL) real
+  const ClLayout lay = cl_layout(kFFT, kF32, sizeof(CodeT) == 2, R1, a.log2b, a.SA, a.SB);
+  C* buf0 = reinterpret_cast<C*>(sm + lay.buf);        // FFT: PL complex
+  Real* xs0 = reinterpret_cast<Real*>(sm + lay.buf);   // FWHT: x: PL, y: PL real
   C* postLo = reinterpret_cast<C*>(sm + lay.post);     // FFT: w_M^{n r2} = postHi[n >> 7] postLo[n & 127]
   C* postHi = postLo + 128;
   C* preHi = reinterpret_cast<C*>(sm + lay.pre);       // FFT, R1 > 1: w_b^{x}, x = hi * 512 + lo
@@ -316,9 +327,57 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
     }
   }
 
-  unsigned step = 0;  // inner indices processed by this CTA (selects the buffer)
+  // the local buffer is cleared once: the scatter writes into it, and the
+  // last radix pass of every inner index leaves it zero again
+  if (kFFT) {
+    for (int e = tid; e < PL; e += kCT) buf0[e] = mk((Real)0, (Real)0);
+  } else {
+    for (int e = tid; e < 2 * PL; e += kCT) xs0[e] = (Real)0;
+  }
+  C* const buf = buf0;
+  Real* const xs = xs0;
+  Real* const ys = xs0 + PL;
+  // exchange slots of this CTA's group in global memory (L2-resident):
+  // [parity][R2][L] elements, parity = step & 1
+  C* const xgr = reinterpret_cast<C*>(a.xch) + (size_t)blockIdx.y * 2 * (size_t)R2 * L;
+
+  // ---- group barrier of the R2 CTAs of one slab.  The grid is a
+  // cooperative launch, so every CTA is resident and every group member
+  // arrives.  Each CTA adds 1 to its group's counter per inner index (after
+  // its exchange writes); the wait of step s needs R2 (s + 1) arrivals.  A
+  // wait that runs out of spins sets the host-mapped flag, and this CTA
+  // skips its later waits (it still arrives) and writes NaN partials, so the
+  // launch ends in bounded time and the failure is visible.
+  unsigned* const gcnt = a.gsync + (size_t)blockIdx.y * 32;
+  __shared__ int s_abort;
+  if (tid == 0) s_abort = 0;
+  auto group_arrive = [&]() {
+    __syncthreads();  // this CTA's exchange writes are issued
+    if (tid == 0) {
+      __threadfence();
+      atomicAdd(gcnt, 1u);
+    }
+  };
+  auto group_wait = [&](unsigned target) {
+    if (tid == 0 && !s_abort) {
+      unsigned spins = 0;
+      while (ld_acquire_gpu(gcnt) < target) {
+        if (++spins > a.spin_limit) {
+          s_abort = 1;
+          *a.timeout = 1;
+          __threadfence_system();
+          break;
+        }
+        __nanosleep(64);
+      }
+      __threadfence();
+    }
+    __syncthreads();  // the other CTAs' exchange writes are visible
+  };
+
+  unsigned step = 0;  // inner indices processed by this CTA (selects the exchange slots)
   // ---- persistent loop over work items (r1, t, k-group); every CTA of a
-  // cluster has the same blockIdx.y, hence the same items and barriers
+  // group has the same blockIdx.y, hence the same items and barriers
   const int items = (R1 * a.d) * a.G;
   for (int item = blockIdx.y; item < items; item += gridDim.y) {
   const int r1 = item & (R1 - 1);
@@ -385,7 +444,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
   const int64_t kb = (int64_t)g * per;
   const int64_t ke = kb + per < a.kc ? kb + per : a.kc;
   // the next inner index with a nonzero row pair (all-zero rows are skipped
-  // identically by every CTA of the cluster)
+  // identically by every CTA of the group)
   auto next_k = [&](int64_t k) -> int64_t {
     if (kFFT)
       while (k < ke && __ldg(a.scale_exp + a.k0 + k) == kCSkip) ++k;
@@ -405,41 +464,23 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
       if (kF32) cp_async4(stB + spad<Real>(e), rB + e); else cp_async8(stB + spad<Real>(e), rB + e);
     }
   };
-  int64_t kk = next_k(kb);
-  if (kk < ke) stage(kk);
-  cluster.sync();  // tables and codes written; the previous item's reads are done
 
-#ifdef CMM_PHASE_CLOCKS
-  long long t_ph = 0;
-#endif
-  while (kk < ke) {
-    CL_MARK(-1);
-    const int64_t kn = next_k(kk + 1);
+  // ---- scatter the staged row k into the (zero) local buffer.  The plan
+  // cuts the segment at bucket boundaries, so every bucket has one writer
+  // thread; its slots are sorted by bucket.  Per batch of kCBatch slots a
+  // thread loads every target first, sums runs of equal buckets in registers
+  // and stores once per run.  The scale is a power of two, applied per value.
+  // Side A and side B write different words when the DIF weights are real
+  // (FFT with R1 <= 2: real / imaginary part; FWHT: x / y), so both sides
+  // run at once.  Ends with a barrier: the buffer is complete and the staged
+  // row is free.
+  auto scatter = [&](int64_t k) {
     Real alpha = (Real)1, beta = (Real)1;
     if (kFFT) {
-      const int se = __ldg(a.scale_exp + a.k0 + kk);
+      const int se = __ldg(a.scale_exp + a.k0 + k);
       alpha = kF32 ? (Real)__int_as_float((127 - se) << 23) : (Real)__longlong_as_double((long long)(1023 - se) << 52);
       beta = kF32 ? (Real)__int_as_float((127 + se) << 23) : (Real)__longlong_as_double((long long)(1023 + se) << 52);
     }
-    C* buf = buf0 + (NB == 2 ? (size_t)(step & 1) * PL : 0);
-    Real* xs = xs0 + (NB == 2 ? (size_t)(step & 1) * 2 * PL : 0);
-    Real* ys = xs + PL;
-    if (kFFT) {
-      for (int e = tid; e < PL; e += kCT) buf[e] = mk((Real)0, (Real)0);
-    } else {
-      for (int e = tid; e < PL; e += kCT) { xs[e] = (Real)0; ys[e] = (Real)0; }
-    }
-    CL_MARK(0);
-    cp_async_wait_all();  // this thread's copies of row kk; the barrier publishes all
-    __syncthreads();
-    CL_MARK(1);
-    // ---- scatter this CTA's residue segment.  The plan cuts the segment at
-    // bucket boundaries, so every bucket has one writer thread; its slots are
-    // sorted by bucket.  Per batch of kCBatch slots a thread loads every
-    // target first, sums runs of equal buckets in registers and stores once
-    // per run.  The scale is a power of two, applied per value.  Side A and
-    // side B write different words when the DIF weights are real (FFT with
-    // R1 <= 2: real / imaginary part; FWHT: x / y), so both sides run at once.
     const bool split = !kFFT || R1 <= 2;
 #pragma unroll
     for (int side = 0; side < 2; ++side) {
@@ -509,14 +550,16 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
       }
       if (side == 0 && !split) __syncthreads();
     }
-    __syncthreads();         // the scatter is done with the staged row
-    CL_MARK(2);
-    if (kn < ke) stage(kn);  // overlaps the transform and the combine
+    __syncthreads();  // the buffer is complete; the staged row is free
+  };
 
-    // ---- local transform of length L (results stay in shared memory)
+  // ---- local transform of length L in shared memory.  The last pass
+  // writes the sub-spectrum to this CTA's exchange slot xo (natural order;
+  // FWHT: (x, y) pairs) and zeros to the buffer.
+  auto transform = [&](C* __restrict__ xo) {
     if (kFFT && !kF32) {
       // 4 radix-8 DIT passes; pass 0 (constant twiddles) applies the DIF
-      // weight w_b^{n1 r1}, pass 3 the post-twiddle w_M^{n r2}
+      // weight w_b^{n1 r1} (r1 > 0), pass 3 the post-twiddle w_M^{n r2}
 #pragma unroll
       for (int ps = 0; ps < 4; ++ps) {
         const int s0 = 3 * ps, half = 1 << s0;
@@ -526,7 +569,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
 #pragma unroll
         for (int e = 0; e < 8; ++e) x[e] = buf[phys<ES>(base + e * half)];
         if (ps == 0) {
-          if (R1 > 1) {
+          if (r1 > 0) {
 #pragma unroll
             for (int e = 0; e < 8; ++e) {
               const uint32_t m = __brev((uint32_t)(base + e)) >> (32 - LOGL);
@@ -540,11 +583,16 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
         }
         if (ps == 3) {
 #pragma unroll
-          for (int e = 0; e < 8; ++e) x[e] = cmul(x[e], post(base + e * half));
-        }
+          for (int e = 0; e < 8; ++e) {
+            const int n = base + e * half;
+            __stcg(xo + n, r2 > 0 ? cmul(x[e], post(n)) : x[e]);
+            buf[phys<ES>(n)] = mk((Real)0, (Real)0);
+          }
+        } else {
 #pragma unroll
-        for (int e = 0; e < 8; ++e) buf[phys<ES>(base + e * half)] = x[e];
-        if (ps < 3) __syncthreads();
+          for (int e = 0; e < 8; ++e) buf[phys<ES>(base + e * half)] = x[e];
+          __syncthreads();
+        }
       }
     } else if (kFFT) {
       // FP32, L = 8192: radix-16 (stages 0-3) + 3 radix-8 passes
@@ -553,7 +601,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
         C x[16];
 #pragma unroll
         for (int e = 0; e < 16; ++e) x[e] = buf[phys<ES>(base + e)];
-        if (R1 > 1) {
+        if (r1 > 0) {
 #pragma unroll
           for (int e = 0; e < 16; ++e) {
             const uint32_t m = __brev((uint32_t)(base + e)) >> (32 - LOGL);
@@ -597,10 +645,15 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
           r8(x, ptw[(ps == 1 ? 0 : (ps == 2 ? 16 : 144)) + kk2]);
           if (ps == 3) {
 #pragma unroll
-            for (int e = 0; e < 8; ++e) x[e] = cmul(x[e], post(base + e * half));
-          }
+            for (int e = 0; e < 8; ++e) {
+              const int n = base + e * half;
+              __stcg(xo + n, r2 > 0 ? cmul(x[e], post(n)) : x[e]);
+              buf[phys<ES>(n)] = mk((Real)0, (Real)0);
+            }
+          } else {
 #pragma unroll
-          for (int e = 0; e < 8; ++e) buf[phys<ES>(base + e * half)] = x[e];
+            for (int e = 0; e < 8; ++e) buf[phys<ES>(base + e * half)] = x[e];
+          }
         }
         if (ps < 3) __syncthreads();
       }
@@ -629,8 +682,18 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
           for (int e = 0; e < 8; ++e) { x[e] = xs[phys<ES>(base + e * half)]; y[e] = ys[phys<ES>(base + e * half)]; }
           whtr<Real, 8>(x);
           whtr<Real, 8>(y);
+          if (ps == 3) {
 #pragma unroll
-          for (int e = 0; e < 8; ++e) { xs[phys<ES>(base + e * half)] = x[e]; ys[phys<ES>(base + e * half)] = y[e]; }
+            for (int e = 0; e < 8; ++e) {
+              const int n = base + e * half;
+              __stcg(xo + n, mk(x[e], y[e]));
+              xs[phys<ES>(n)] = (Real)0;
+              ys[phys<ES>(n)] = (Real)0;
+            }
+          } else {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) { xs[phys<ES>(base + e * half)] = x[e]; ys[phys<ES>(base + e * half)] = y[e]; }
+          }
         }
         if (ps < 3) __syncthreads();
       }
@@ -652,30 +715,31 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
         const int m = tid + kCT * e;
         const float x0 = fx[phys<ES>(m)], x1 = fx[phys<ES>(m + 4096)];
         const float y0 = fy[phys<ES>(m)], y1 = fy[phys<ES>(m + 4096)];
-        fx[phys<ES>(m)] = x0 + x1; fx[phys<ES>(m + 4096)] = x0 - x1;
-        fy[phys<ES>(m)] = y0 + y1; fy[phys<ES>(m + 4096)] = y0 - y1;
+        __stcg(xo + m, mk((Real)(x0 + x1), (Real)(y0 + y1)));
+        __stcg(xo + m + 4096, mk((Real)(x0 - x1), (Real)(y0 - y1)));
+        fx[phys<ES>(m)] = 0.f; fx[phys<ES>(m + 4096)] = 0.f;
+        fy[phys<ES>(m)] = 0.f; fy[phys<ES>(m + 4096)] = 0.f;
       }
     }
+  };
 
-    CL_MARK(3);
-    cluster.sync();  // every sub-spectrum of the cluster is complete
-    CL_MARK(4);
-
-    // ---- radix-R2 combine across the cluster; accumulate.  With R2 = 16 the
-    // two threads of a lane pair own the even / odd outputs of one position:
-    // each reads half of the 16 sub-spectra and they swap halves by shuffle.
+  // ---- radix-R2 combine of the group's sub-spectra, read back from the
+  // exchange slots xst of this step; accumulate.  With R2 = 16 the two
+  // threads of a lane pair own the even / odd outputs of one position: each
+  // reads half of the 16 sub-spectra and they swap halves by shuffle.
+  auto combine = [&](const C* __restrict__ xst) {
 #pragma unroll
     for (int u = 0; u < OUT / 8; ++u) {
       const int gi = tid + kCT * u;
       const int nl = gi >> (a.logR2 - 3);
       const int half = gi & ((R2 >> 3) - 1);
       const int n = r2 * (L >> a.logR2) + nl;
-      if (kFFT) {
-        C z[8];
-        if (R2 == 16) {
-          const int rb = half ? 8 : 0;
+      const int rb = (R2 == 16 && half) ? 8 : 0;
+      C z[8];
 #pragma unroll
-          for (int r = 0; r < 8; ++r) z[r] = cluster.map_shared_rank(buf, rb + r)[phys<ES>(n)];
+      for (int r = 0; r < 8; ++r) z[r] = __ldcg(xst + (size_t)(rb + r) * L + n);
+      if (kFFT) {
+        if (R2 == 16) {
 #pragma unroll
           for (int r = 0; r < 8; ++r) {
             const C o = mk(__shfl_xor_sync(0xffffffffu, z[r].x, 1), __shfl_xor_sync(0xffffffffu, z[r].y, 1));
@@ -683,9 +747,6 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
             if (half == 0) z[r] = mk(z[r].x + o.x, z[r].y + o.y);
             else z[r] = cmul(mk(o.x - z[r].x, o.y - z[r].y), ptw[(kF32 ? 1168 : 584) + r]);
           }
-        } else {
-#pragma unroll
-          for (int r = 0; r < 8; ++r) z[r] = cluster.map_shared_rank(buf, r)[phys<ES>(n)];
         }
         dft8(z);
 #pragma unroll
@@ -703,24 +764,14 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
         }
       } else {
         Real zx[8], zy[8];
-        if (R2 == 16) {
-          const int rb = half ? 8 : 0;
 #pragma unroll
-          for (int r = 0; r < 8; ++r) {
-            zx[r] = cluster.map_shared_rank(xs, rb + r)[phys<ES>(n)];
-            zy[r] = cluster.map_shared_rank(ys, rb + r)[phys<ES>(n)];
-          }
+        for (int r = 0; r < 8; ++r) { zx[r] = z[r].x; zy[r] = z[r].y; }
+        if (R2 == 16) {
 #pragma unroll
           for (int r = 0; r < 8; ++r) {
             const Real ox = __shfl_xor_sync(0xffffffffu, zx[r], 1), oy = __shfl_xor_sync(0xffffffffu, zy[r], 1);
             zx[r] = half == 0 ? zx[r] + ox : ox - zx[r];
             zy[r] = half == 0 ? zy[r] + oy : oy - zy[r];
-          }
-        } else {
-#pragma unroll
-          for (int r = 0; r < 8; ++r) {
-            zx[r] = cluster.map_shared_rank(xs, r)[phys<ES>(n)];
-            zy[r] = cluster.map_shared_rank(ys, r)[phys<ES>(n)];
           }
         }
         whtr<Real, 8>(zx);
@@ -733,26 +784,68 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
         }
       }
     }
-    if (NB == 1) cluster.sync();  // all reads of the sub-spectra are done
-    CL_MARK(5);
+  };
+
+  // ---- software pipeline over the inner indices.  On entry to an
+  // iteration row kk is scattered in the buffer and row kn is being staged.
+  // The group barrier of index kk is split: the arrive follows the write of
+  // the sub-spectrum, the wait precedes the combine, and the scatter of row
+  // kn runs in between.  The exchange slots are double-buffered by the
+  // parity of the step: the barrier of step i orders every CTA's reads of
+  // step i - 1 before the writes of step i + 1.
+  int64_t kk = next_k(kb);
+  int64_t kn = ke;
+  if (kk < ke) {
+    stage(kk);
+    cp_async_wait_all();
+    __syncthreads();
+    scatter(kk);
+    kn = next_k(kk + 1);
+    if (kn < ke) stage(kn);
+  }
+#ifdef CMM_PHASE_CLOCKS
+  long long t_ph = 0;
+#endif
+  while (kk < ke) {
+    CL_MARK(-1);
+    C* const xst = xgr + (size_t)(step & 1) * R2 * L;
+    transform(xst + (size_t)r2 * L);
+    group_arrive();
+    CL_MARK(0);
+    int64_t k2 = ke;
+    if (kn < ke) {
+      cp_async_wait_all();  // this thread's copies of row kn; the barrier publishes all
+      __syncthreads();
+      CL_MARK(1);
+      scatter(kn);
+      CL_MARK(2);
+      k2 = next_k(kn + 1);
+      if (k2 < ke) stage(k2);  // overlaps the combine and the next transform
+    }
+    group_wait((unsigned)R2 * (step + 1u) + a.wait_extra);
+    CL_MARK(3);
+    combine(xst);
+    CL_MARK(4);
 #ifdef CMM_PHASE_CLOCKS
     if (tid == 0) atomicAdd(&g_cl_phase[kClPhases], 1ull);
 #endif
     ++step;
     kk = kn;
+    kn = k2;
   }
 
+  const bool bad = s_abort != 0;  // written before the barrier that ends this item's last wait
 #pragma unroll
   for (int o = 0; o < OUT; ++o) {
     const int gi = tid + kCT * (o >> 3);
     const int64_t f = out_f(gi, o & 7);
-    const double vx = kF32 ? (double)qh[o][0] + (double)ql[o][0] : qd[o][0];
-    const double vy = kF32 ? (double)qh[o][QC - 1] + (double)ql[o][QC - 1] : qd[o][QC - 1];
+    double vx = kF32 ? (double)qh[o][0] + (double)ql[o][0] : qd[o][0];
+    double vy = kF32 ? (double)qh[o][QC - 1] + (double)ql[o][QC - 1] : qd[o][QC - 1];
+    if (bad) vx = vy = __longlong_as_double(0x7ff8000000000000ll);
     if (kFFT) partC[f] = make_double2(vx, vy);
     else partR[f] = vx;
   }
   }  // item loop
-  if (NB == 2) cluster.sync();  // the other CTAs' last reads of this CTA's buffers
 }
 
 // ------------------------------------------------------------------ host
@@ -785,70 +878,73 @@ bool sketch_cluster_applicable(int variant, bool f32, int b) {
   return log2b - logL >= 3 && log2b <= 19;  // R >= 8; DIF twiddle table covers b <= 2^19
 }
 
-constexpr size_t kClSmemMax = 227 * 1024;
+constexpr size_t kClSmemMax = 227 * 1024 - 64;  // less the kernel's static shared bytes
 
-template <int V, typename Real, typename CodeT, int NB>
+template <int V, typename Real, typename CodeT>
 static void cl_kernel_attrs(size_t smem) {
-  auto k = k_sketch_cluster<V, Real, CodeT, NB>;
-  CMM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  CMM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  CMM_CUDA(cudaFuncSetAttribute(k_sketch_cluster<V, Real, CodeT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem));
 }
 
-// shared bytes of one CTA and the buffer count: two sub-spectrum buffers
-// when they fit, else one
-static size_t cl_smem(int variant, bool f32, bool u16, int R1, int log2b, int64_t SA, int64_t SB, int* nb) {
-  const bool fft = variant == kVariantFFT;
-  const size_t two = cl_layout(fft, f32, u16, 2, R1, log2b, SA, SB).total;
-  if (two <= kClSmemMax) {
-    if (nb) *nb = 2;
-    return two;
-  }
-  if (nb) *nb = 1;
-  return cl_layout(fft, f32, u16, 1, R1, log2b, SA, SB).total;
+// shared bytes of one CTA
+static size_t cl_smem(int variant, bool f32, bool u16, int R1, int log2b, int64_t SA, int64_t SB) {
+  return cl_layout(variant == kVariantFFT, f32, u16, R1, log2b, SA, SB).total;
 }
 
-template <int V, typename Real, typename CodeT, int NB>
-static void cl_launch(const ClArgs& a, dim3 grid, int R2, size_t smem, cudaStream_t s) {
+// cooperative launch: the group barriers need every CTA resident
+template <int V, typename Real, typename CodeT>
+static void cl_launch(const ClArgs& a, dim3 grid, size_t smem, cudaStream_t s) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = dim3(kCT, 1, 1);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = (unsigned)R2;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  CMM_CUDA(cudaLaunchKernelEx(&cfg, k_sketch_cluster<V, Real, CodeT, NB>, a));
+  CMM_CUDA(cudaLaunchKernelEx(&cfg, k_sketch_cluster<V, Real, CodeT>, a));
 }
 
+// CTAs resident on the whole device at this shared-memory size
 template <int V, typename Real, typename CodeT>
-static int cl_max_clusters(int R2, size_t smem) {
-  cl_kernel_attrs<V, Real, CodeT, 1>(smem);
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)R2, 1, 1);
-  cfg.blockDim = dim3(kCT, 1, 1);
-  cfg.dynamicSmemBytes = smem;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = (unsigned)R2;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  int n = 0;
-  if (cudaOccupancyMaxActiveClusters(&n, k_sketch_cluster<V, Real, CodeT, 1>, &cfg) != cudaSuccess) {
+static int cl_resident(size_t smem) {
+  cl_kernel_attrs<V, Real, CodeT>(smem);
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sketch_cluster<V, Real, CodeT>, kCT, smem) !=
+      cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
-  return n;
+  return per_sm * num_sms();
 }
 
-// Chooses R2 in {16, 8} and the k-group count G from the number of
-// co-resident clusters NC: the grid holds NC persistent clusters that share
-// the R1 * d * G work items round-robin; the estimate ceil(items/NC)/G is
+// host-mapped flag set by a group wait that ran out of spins
+static int* group_timeout_flag(int** dev) {
+  static int* host = nullptr;
+  static int* mapped = nullptr;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> g(mu);
+  if (!host) {
+    CMM_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&host), sizeof(int), cudaHostAllocMapped));
+    *host = 0;
+    CMM_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&mapped), host, 0));
+  }
+  if (dev) *dev = mapped;
+  return host;
+}
+
+bool sketch_group_timed_out() {
+  volatile int* h = group_timeout_flag(nullptr);
+  const bool t = *h != 0;
+  *h = 0;
+  return t;
+}
+
+// Chooses R2 in {16, 8} and the k-group count G from the number of groups
+// NG = resident CTAs / R2: the grid holds NG persistent groups that share
+// the R1 * d * G work items round-robin; the estimate ceil(items/NG)/G is
 // minimised (ties to R2 = 16: less scatter redundancy, fewer items).
 ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, int64_t est_slots) {
   ClusterPlan C;
@@ -860,12 +956,13 @@ ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, i
   for (int logR2 : {4, 3}) {
     if (logR2 > logR) continue;
     const int R2 = 1 << logR2, R1 = 1 << (logR - logR2);
-    const size_t smem = cl_smem(variant, f32, true, R1, C.log2b, est_slots, est_slots, nullptr);
-    int mx;
+    const size_t smem = cl_smem(variant, f32, true, R1, C.log2b, est_slots, est_slots);
+    int ctas;
     if (variant == kVariantFFT)
-      mx = f32 ? cl_max_clusters<0, float, uint16_t>(R2, smem) : cl_max_clusters<0, double, uint16_t>(R2, smem);
+      ctas = f32 ? cl_resident<0, float, uint16_t>(smem) : cl_resident<0, double, uint16_t>(smem);
     else
-      mx = f32 ? cl_max_clusters<1, float, uint16_t>(R2, smem) : cl_max_clusters<1, double, uint16_t>(R2, smem);
+      ctas = f32 ? cl_resident<1, float, uint16_t>(smem) : cl_resident<1, double, uint16_t>(smem);
+    const int mx = ctas / R2;
     if (mx <= 0) continue;
     const int64_t base = (int64_t)R1 * d;
     for (int64_t G = 1; G <= 64; ++G) {
@@ -873,7 +970,7 @@ ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, i
       if (base * G > 65535) break;
       const int64_t items = base * G;
       const int64_t nc = items < mx ? items : mx;
-      // per-cluster load in units of one (r1, t) over all k; scatter cost ~R1
+      // per-group load in units of one (r1, t) over all k; scatter cost ~R1
       const double load = (double)((items + nc - 1) / nc) / (double)G * (1.0 + 0.05 * R1);
       if (load < best - 1e-9) {
         best = load;
@@ -884,15 +981,15 @@ ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, i
       }
     }
   }
-  if (best >= 1e299) throw unsupported("no cluster configuration fits this device");
+  if (best >= 1e299) throw unsupported("no group configuration fits this device");
   if (getenv("CMM_DEBUG"))
-    fprintf(stderr, "[cmm] cluster plan: b=%d L=%d R1=%d R2=%d G=%d clusters=%d\n", b, 1 << C.logL,
+    fprintf(stderr, "[cmm] group plan: b=%d L=%d R1=%d R2=%d G=%d groups=%d\n", b, 1 << C.logL,
             1 << C.logR1, 1 << C.logR2, C.G, C.max_clusters);
   return C;
 }
 
 bool cluster_smem_fits(int variant, bool f32, const ClusterPlan& C, const SlabPlan& P) {
-  return cl_smem(variant, f32, P.u16, 1 << C.logR1, C.log2b, P.EA, P.EB, nullptr) <= kClSmemMax;
+  return cl_smem(variant, f32, P.u16, 1 << C.logR1, C.log2b, P.EA, P.EB) <= kClSmemMax;
 }
 
 void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const SlabPlan& P,
@@ -920,24 +1017,36 @@ void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const Sl
   a.G = C.G;
   a.accumulate = accumulate;
   const int R2 = 1 << C.logR2, R1 = 1 << C.logR1;
-  int nb = 1;
-  const size_t smem = cl_smem(variant, f32, P.u16, R1, C.log2b, a.SA, a.SB, &nb);
+  const size_t smem = cl_smem(variant, f32, P.u16, R1, C.log2b, a.SA, a.SB);
   if (smem > kClSmemMax) throw unsupported("cluster sketch: residue segments too large for shared memory");
+  if (sketch_group_timed_out())
+    throw std::runtime_error("cluster sketch: a group barrier wait ran out in an earlier launch");
+  // exchange area: two parities of R2 sub-spectra of L elements per group;
+  // group counters: one 128-byte line each
+  const size_t elem = f32 ? 8 : 16;
+  const int groups = C.max_clusters;
+  DevBuf xch((size_t)groups * 2 * (size_t)R2 * ((size_t)1 << C.logL) * elem, s);
+  DevBuf gsync((size_t)groups * 128, s);
+  CMM_CUDA(cudaMemsetAsync(gsync.ptr, 0, gsync.bytes, s));
+  a.xch = xch.ptr;
+  a.gsync = gsync.as<unsigned>();
+  group_timeout_flag(&a.timeout);
+  a.spin_limit = 1u << 24;  // over a second of 64 ns sleeps; a step takes microseconds
+  a.wait_extra = 0;
+  if (const char* e = getenv("CMM_TEST_GROUP_WAIT_EXTRA")) {  // test hook: waits that cannot complete
+    a.wait_extra = (unsigned)atoi(e);
+    if (a.wait_extra) a.spin_limit = 2000;
+  }
   if (getenv("CMM_DEBUG"))
-    fprintf(stderr, "[cmm] cluster launch: smem=%zu buffers=%d SA=%lld SB=%lld\n", smem, nb, (long long)a.SA,
-            (long long)a.SB);
-  const dim3 grid((unsigned)R2, (unsigned)C.max_clusters, 1);
+    fprintf(stderr, "[cmm] group launch: smem=%zu SA=%lld SB=%lld groups=%d exchange=%zu bytes\n", smem,
+            (long long)a.SA, (long long)a.SB, groups, xch.bytes);
+  const dim3 grid((unsigned)R2, (unsigned)groups, 1);
   ProfScope prof("sketch", s);
   count_launch();
-#define CMM_CL(V, T, CT)                                  \
-  do {                                                     \
-    if (nb == 2) {                                         \
-      cl_kernel_attrs<V, T, CT, 2>(smem);                  \
-      cl_launch<V, T, CT, 2>(a, grid, R2, smem, s);        \
-    } else {                                               \
-      cl_kernel_attrs<V, T, CT, 1>(smem);                  \
-      cl_launch<V, T, CT, 1>(a, grid, R2, smem, s);        \
-    }                                                      \
+#define CMM_CL(V, T, CT)                   \
+  do {                                     \
+    cl_kernel_attrs<V, T, CT>(smem);       \
+    cl_launch<V, T, CT>(a, grid, smem, s); \
   } while (0)
   if (variant == kVariantFFT) {
     if (f32) { if (P.u16) CMM_CL(0, float, uint16_t); else CMM_CL(0, float, uint32_t); }

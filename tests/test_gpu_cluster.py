@@ -2,13 +2,13 @@
 
 The shapes are chosen so that the automatic dispatch takes the cluster
 kernels (asserted through cmm_last_sketch_kernel) and cover:
-  * clusters of 16 (radix-16 combine split over lane pairs) and of 8;
+  * groups of 16 CTAs (radix-16 combine split over lane pairs) and of 8;
   * R1 <= 2 (real DIF weights: the two sides scatter into the real and
     imaginary parts at once) and R1 > 2 (complex weights, sides one after
     the other);
-  * two sub-spectrum buffers (FFT) and one (FP64 FWHT);
-  * several work items per cluster and several k-groups;
-  * all-zero rows, which every CTA of a cluster skips, including at the
+  * the sub-spectra exchanged through global memory, double-buffered;
+  * several work items per group and several k-groups;
+  * all-zero rows, which every CTA of a group skips, including at the
     start and end of the inner range (the staged next row must follow);
   * chunked materialization (accumulating launches), on device inputs and
     on streamed host rows;
@@ -132,3 +132,18 @@ def test_fft_mixed(gpu, oracle, b):
     AT = rng.standard_normal((31, 240))
     B = rng.standard_normal((31, 220)) * 1e3
     check("fft", "multiply shift", AT, B, 3, b, 5, oracle, f32=True)
+
+
+def test_group_wait_that_runs_out_is_reported(gpu, oracle, monkeypatch):
+    """A group barrier wait is bounded: with the test hook every wait needs
+    one arrival more than the group makes, so each CTA gives up after a
+    short spin, the launch ends, its partials are NaN and the synchronous
+    entry point raises.  The next product is unaffected."""
+    rng = np.random.default_rng(77)
+    AT = rng.standard_normal((20, 120))
+    B = rng.standard_normal((20, 110))
+    monkeypatch.setenv("CMM_TEST_GROUP_WAIT_EXTRA", "1")
+    with pytest.raises(RuntimeError, match="group barrier wait ran out"):
+        capi().compressed_product("fft", None, AT, B, 3, 1 << 16, 9)
+    monkeypatch.delenv("CMM_TEST_GROUP_WAIT_EXTRA")
+    check("fft", None, AT, B, 3, 1 << 16, 9, oracle)
