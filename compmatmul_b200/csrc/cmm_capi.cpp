@@ -300,11 +300,10 @@ static bool try_cluster_plan(int variant, bool f32, const Codes& codes, int64_t 
                              cudaStream_t s) {
   if (!sketch_cluster_applicable(variant, f32, sp.b)) return false;
   if (sketch_kernel_choice() == 2) return false;
-  // auto: measured on B200 at n = 16384, d = 9 -- the cluster kernels win
-  // for every FFT case and for FP64 FWHT (167.7 against 176-188 ms per
-  // product at b = 2^16); the tensor-core slab kernel wins for FP32 FWHT
-  // (513 against 545 ms of sketch kernel at b = 2^18)
-  if (sketch_kernel_choice() == 0 && variant == kVariantFWHT && f32) return false;
+  // auto: measured on B200 at n = 16384, d = 9 -- the group kernels win
+  // for every FFT case, for FP64 FWHT (86.6 against 176-188 ms of sketch
+  // kernel per product at b = 2^16 on the slab kernel) and for FP32 FWHT
+  // (351 against 509 ms at b = 2^18 on the tensor-core slab kernel)
   try {
     C = plan_cluster(variant, f32, n_inner, sp.d, sp.b, 4096);
   } catch (const unsupported&) {

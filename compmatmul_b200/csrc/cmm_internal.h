@@ -218,6 +218,7 @@ void launch_f32_to_f64(const float* src, double* dst, int64_t n, cudaStream_t s)
 // natural frequency order [g][t][b].
 struct ClusterPlan {
   int logL = 0, log2b = 0, logR1 = 0, logR2 = 0, G = 1, max_clusters = 0;
+  int nt = 512;  // threads per CTA: 512, or 256 (FP64, two CTAs per SM)
 };
 bool sketch_cluster_applicable(int variant, bool f32, int b);
 ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, int64_t est_slots);

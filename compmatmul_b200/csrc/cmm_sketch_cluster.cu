@@ -13,17 +13,18 @@
 //  * the R2 sub-spectra are combined by a radix-R2 DFT/WHT across the
 //    group: the last radix pass writes each CTA's sub-spectrum to an
 //    exchange area in global memory, which stays in L2 (R2 x L elements per
-//    group, double-buffered), and after the group barrier CTA r2 reads the
+//    group, four slots in rotation), and after the group barrier CTA r2 reads the
 //    R2 values of its L / R2 sub-spectrum positions back and accumulates
 //    Z^2 (FFT, z = alpha x + i beta y) or X * Y (FWHT) for them over k.
 //    Thread-block clusters exchanging through distributed shared memory were
 //    the earlier form: clusters of 8 fit 15 times on the 148 SMs, and the
 //    remote reads ran at about a third of their port's peak.
 //  The grid is one cooperative launch of every resident CTA, in groups of
-//  R2; a group barrier is a counter in global memory.  It is split (arrive
-//  after the exchange write, wait before the combine) and the next row's
-//  scatter runs in between; the row after that is staged with cp.async
-//  while the current one is combined and transformed.  Every CTA of a group
+//  R2; a group barrier is a counter in global memory.  It is split: a CTA
+//  arrives for index k after its exchange write and the next row's scatter,
+//  and waits for k one iteration later, after the transform of k + 1 and
+//  the scatter of k + 2, so the combine of k runs behind the transform of
+//  k + 1; the row after that is staged with cp.async meanwhile.  Every CTA of a group
 //  runs the same k sequence (all-zero rows are skipped by all of them), so
 //  all of them reach every barrier.
 // Instantiations: FFT/FWHT x FP64/FP32 (FP32 = mixed precision: FP32 data,
@@ -77,10 +78,17 @@ __device__ __forceinline__ uint32_t bf16x2(float lo_e, float hi_e) {
   return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(lo_e)) |
          ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(hi_e)) << 16);
 }
-__device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_t& lo) {
+// x = hi + mid + lo in BF16 (8 + 8 + 8 significant bits cover FP32's 24),
+// so the +-1 products on the tensor cores lose nothing before the FP32
+// accumulation (a hi/lo split measured 1.02e-5 max relative error on the
+// recovered values of a 16384^2, b = 2^18 product)
+__device__ __forceinline__ void split3(float x0, float x1, uint32_t& hi, uint32_t& mid, uint32_t& lo) {
   const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
+  const float r0 = x0 - __bfloat162float(h0), r1 = x1 - __bfloat162float(h1);
+  const __nv_bfloat16 m0 = __float2bfloat16_rn(r0), m1 = __float2bfloat16_rn(r1);
   hi = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
-  lo = bf16x2(x0 - __bfloat162float(h0), x1 - __bfloat162float(h1));
+  mid = (uint32_t)__bfloat16_as_ushort(m0) | ((uint32_t)__bfloat16_as_ushort(m1) << 16);
+  lo = bf16x2(r0 - __bfloat162float(m0), r1 - __bfloat162float(m1));
 }
 __device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
   asm volatile(
@@ -107,14 +115,16 @@ __device__ __forceinline__ void h16(float* buf, const uint32_t (&hb)[2][2], int 
     float x[8];
 #pragma unroll
     for (int e = 0; e < 8; ++e) x[e] = buf[phys<4>(p[e])];
-    uint32_t ahi[4], alo[4];
+    uint32_t ahi[4], amid[4], alo[4];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) split2(x[2 * e], x[2 * e + 1], ahi[e], alo[e]);
+    for (int e = 0; e < 4; ++e) split3(x[2 * e], x[2 * e + 1], ahi[e], amid[e], alo[e]);
     float c0[4] = {0.f, 0.f, 0.f, 0.f}, c1[4] = {0.f, 0.f, 0.f, 0.f};
+    mma16816(c0, alo, hb[0][0], hb[0][1]);  // smallest parts first
+    mma16816(c0, amid, hb[0][0], hb[0][1]);
     mma16816(c0, ahi, hb[0][0], hb[0][1]);
-    mma16816(c0, alo, hb[0][0], hb[0][1]);
-    mma16816(c1, ahi, hb[1][0], hb[1][1]);
     mma16816(c1, alo, hb[1][0], hb[1][1]);
+    mma16816(c1, amid, hb[1][0], hb[1][1]);
+    mma16816(c1, ahi, hb[1][0], hb[1][1]);
     const float y[8] = {c0[0], c0[1], c0[2], c0[3], c1[0], c1[1], c1[2], c1[3]};
 #pragma unroll
     for (int e = 0; e < 8; ++e) buf[phys<4>(p[e])] = y[e];
@@ -128,9 +138,9 @@ __device__ __forceinline__ void h16(float* buf, const uint32_t (&hb)[2][2], int 
 // CMM_EXTRA_NVFLAGS=-DCMM_PHASE_CLOCKS): thread 0 of every CTA adds the
 // clock64() time of each phase of each inner index to g_cl_phase, which
 // cmm_cluster_phase_cycles() reads and clears.  Phases: 0 the local radix
-// passes with the write of the sub-spectrum and the arrival, 1 wait for the
-// next staged row (cp.async + barrier), 2 its scatter, 3 the rest of the
-// group barrier (wait), 4 the combine and accumulation; 5 is unused.
+// passes with the write of the sub-spectrum, 1 wait for the next staged row
+// (cp.async + barrier), 2 its scatter, 3 the arrival and the group wait for
+// the previous index, 4 the combine and accumulation; 5 is unused.
 constexpr int kClPhases = 6;
 #ifdef CMM_PHASE_CLOCKS
 __device__ unsigned long long g_cl_phase[kClPhases + 1];  // + inner indices timed
@@ -158,8 +168,8 @@ struct ClArgs {
   const int* scale_exp;
   const double2* tw;  // w_b^j
   void* partial;      // [g][t][b] double2 (FFT) / double (FWHT)
-  void* xch;          // exchange area: [group][2][R2][L] complex (FFT) / (x, y) pairs (FWHT)
-  unsigned* gsync;    // arrival counters, one 128-byte line per group, zero at launch
+  void* xch;          // exchange area: [group][4][R2][L] complex (FFT) / (x, y) pairs (FWHT)
+  unsigned* gsync;    // arrival counters, 4 per group (one 128-byte line each), zero at launch
   int* timeout;       // host-mapped flag: a group wait ran out
   unsigned spin_limit, wait_extra;
   int64_t SA, SB, kc, k0;
@@ -188,10 +198,10 @@ struct ClLayout {
   size_t buf, post, pre, ptw, wr, stage, codes, total;
 };
 __host__ __device__ inline size_t cl_align16(size_t x) { return (x + 15) & ~(size_t)15; }
-__host__ __device__ inline ClLayout cl_layout(bool fft, bool f32, bool u16, int R1, int log2b,
+__host__ __device__ inline ClLayout cl_layout(bool fft, bool f32, bool u16, int logL, int R1, int log2b,
                                               int64_t SA, int64_t SB) {
   const size_t real = f32 ? 4 : 8, cpx = 2 * real;
-  const size_t L = (fft && !f32) ? 4096 : 8192;
+  const size_t L = (size_t)1 << logL;
   auto plen = [](size_t n, size_t es) { return es == 4 ? n + n / 32 : n + n / 16; };
   ClLayout o;
   size_t p = 0;
@@ -230,18 +240,25 @@ static __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
+static __device__ __forceinline__ void red_release_gpu_add(unsigned* p, unsigned v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
 
-// VARIANT 0 = FFT, 1 = FWHT; Real = double (plain) or float (mixed).
-template <int VARIANT, typename Real, typename CodeT>
-__global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
+// VARIANT 0 = FFT, 1 = FWHT; Real = double (plain) or float (mixed); NT
+// threads per CTA: 512 (one CTA per SM) or, FP64 only, 256 with half the
+// sub-transform length (two CTAs per SM, whose phases overlap).
+template <int VARIANT, typename Real, typename CodeT, int NT>
+__global__ void __launch_bounds__(NT, kCT / NT) k_sketch_cluster(ClArgs a) {
   constexpr bool kFFT = VARIANT == kVariantFFT;
   constexpr bool kF32 = sizeof(Real) == 4;
-  constexpr int LOGL = (kFFT && !kF32) ? 12 : 13;
+  static_assert(NT == kCT || (NT == kCT / 2 && !kF32), "256-thread CTAs are FP64 only");
+  constexpr int LOGL = ((kFFT && !kF32) ? 12 : 13) - (NT == kCT ? 0 : 1);
+  constexpr int VPT = kCT / NT;  // plan ranges (of kCT per segment) per thread
   constexpr int L = 1 << LOGL;
   using C = typename std::conditional<kF32, float2, double2>::type;
   constexpr int ES = kFFT ? (int)sizeof(C) : (int)sizeof(Real);  // shared element size
   constexpr int PL = phys_len<ES>(L);
-  constexpr int OUT = L / kCT;  // outputs per thread (8 or 16)
+  constexpr int OUT = L / NT;  // outputs per thread (8 or 16)
 
   extern __shared__ __align__(16) unsigned char sm[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -251,7 +268,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
   const double2* tw = a.tw;
 
   // ---- shared layout (cl_layout)
-  const ClLayout lay = cl_layout(kFFT, kF32, sizeof(CodeT) == 2, R1, a.log2b, a.SA, a.SB);
+  const ClLayout lay = cl_layout(kFFT, kF32, sizeof(CodeT) == 2, LOGL, R1, a.log2b, a.SA, a.SB);
   C* buf0 = reinterpret_cast<C*>(sm + lay.buf);        // FFT: PL complex
   Real* xs0 = reinterpret_cast<Real*>(sm + lay.buf);   // FWHT: x: PL, y: PL real
   C* postLo = reinterpret_cast<C*>(sm + lay.post);     // FFT: w_M^{n r2} = postHi[n >> 7] postLo[n & 127]
@@ -268,7 +285,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
 
   // ---- tables (constant over k)
   if (kFFT) {
-    for (int e = tid; e < 128 + 64; e += kCT) {
+    for (int e = tid; e < 128 + 64; e += NT) {
       const uint64_t n = e < 128 ? (uint64_t)e : (uint64_t)(e - 128) << 7;
       if (n < (uint64_t)L) {
         const double2 w = tw[(n * (uint64_t)r2) << a.logR1];  // w_M^{n r2} = w_b^{n r2 R1}
@@ -276,12 +293,12 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
       }
     }
     if (R1 > 1) {
-      for (int e = tid; e < cl_pre_hi(a.log2b); e += kCT) {
+      for (int e = tid; e < cl_pre_hi(a.log2b); e += NT) {
         const uint64_t x = (uint64_t)e << 9;
         const double2 w = x < ((uint64_t)1 << a.log2b) ? tw[x] : make_double2(1.0, 0.0);
         preHi[e] = mk((Real)w.x, (Real)w.y);
       }
-      for (int e = tid; e < 512; e += kCT) {
+      for (int e = tid; e < 512; e += NT) {
         const double2 w = tw[e];
         preLo[e] = mk((Real)w.x, (Real)w.y);
       }
@@ -289,15 +306,15 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
     // pass twiddles w_{8 half}^kk at half = 8^p (FP64: 3 passes after the
     // first) or 16 * 8^(p-1) (FP32), and w_16^k for the cluster combine
     if (!kF32) {
-      // [0,8) w_64, [8,72) w_512, [72,584) w_4096, [584,592) w_16
-      for (int e = tid; e < 8 + 64 + 512 + 8; e += kCT) {
-        const int lg = e < 8 ? 6 : (e < 72 ? 9 : (e < 584 ? 12 : 4));
+      // [0,8) w_64, [8,72) w_512, [72,584) w_L, [584,592) w_16
+      for (int e = tid; e < 8 + 64 + 512 + 8; e += NT) {
+        const int lg = e < 8 ? 6 : (e < 72 ? 9 : (e < 584 ? LOGL : 4));
         const int kk = e < 8 ? e : (e < 72 ? e - 8 : (e < 584 ? e - 72 : e - 584));
         const double2 w = tw[(uint32_t)kk << (a.log2b - lg)];
         ptw[e] = mk((Real)w.x, (Real)w.y);
       }
     } else {
-      for (int e = tid; e < 16 + 128 + 1024 + 8; e += kCT) {
+      for (int e = tid; e < 16 + 128 + 1024 + 8; e += NT) {
         int lg, kk;
         if (e < 16) { lg = 7; kk = e; }
         else if (e < 144) { lg = 10; kk = e - 16; }
@@ -307,7 +324,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
         ptw[e] = mk((Real)w.x, (Real)w.y);
       }
     }
-    for (int e = tid; e < 16; e += kCT) {
+    for (int e = tid; e < 16; e += NT) {
       const double2 w = e < R1 ? tw[(uint32_t)e << logM] : make_double2(1.0, 0.0);  // w_R1^e
       wRx[e] = (Real)w.x;
       wRy[e] = (Real)w.y;
@@ -330,38 +347,42 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
   // the local buffer is cleared once: the scatter writes into it, and the
   // last radix pass of every inner index leaves it zero again
   if (kFFT) {
-    for (int e = tid; e < PL; e += kCT) buf0[e] = mk((Real)0, (Real)0);
+    for (int e = tid; e < PL; e += NT) buf0[e] = mk((Real)0, (Real)0);
   } else {
-    for (int e = tid; e < 2 * PL; e += kCT) xs0[e] = (Real)0;
+    for (int e = tid; e < 2 * PL; e += NT) xs0[e] = (Real)0;
   }
   C* const buf = buf0;
   Real* const xs = xs0;
   Real* const ys = xs0 + PL;
   // exchange slots of this CTA's group in global memory (L2-resident):
-  // [parity][R2][L] elements, parity = step & 1
-  C* const xgr = reinterpret_cast<C*>(a.xch) + (size_t)blockIdx.y * 2 * (size_t)R2 * L;
+  // [parity][R2][L] elements, parity = step & 3
+  C* const xgr = reinterpret_cast<C*>(a.xch) + (size_t)blockIdx.y * 4 * (size_t)R2 * L;
 
   // ---- group barrier of the R2 CTAs of one slab.  The grid is a
   // cooperative launch, so every CTA is resident and every group member
-  // arrives.  Each CTA adds 1 to its group's counter per inner index (after
-  // its exchange writes); the wait of step s needs R2 (s + 1) arrivals.  A
-  // wait that runs out of spins sets the host-mapped flag, and this CTA
-  // skips its later waits (it still arrives) and writes NaN partials, so the
-  // launch ends in bounded time and the failure is visible.
-  unsigned* const gcnt = a.gsync + (size_t)blockIdx.y * 32;
+  // arrives.  Each group has one arrival counter per exchange slot (step
+  // mod 4); a CTA adds 1 to the counter of step s after its exchange
+  // writes, and the wait for step s needs R2 (s / 4 + 1) arrivals there.
+  // Counting per slot keeps the wait exact although CTAs drift apart by a
+  // step: an arrival at step s + 4 follows its CTA's wait for step s + 2,
+  // hence every CTA's arrival at step s.  A wait that runs out of spins
+  // sets the host-mapped flag, and this CTA skips its later waits (it still
+  // arrives) and writes NaN partials, so the launch ends in bounded time
+  // and the failure is visible.
+  unsigned* const gcnt = a.gsync + (size_t)blockIdx.y * 128;  // 4 counters, 128 bytes apart
   __shared__ int s_abort;
   if (tid == 0) s_abort = 0;
-  auto group_arrive = [&]() {
-    __syncthreads();  // this CTA's exchange writes are issued
-    if (tid == 0) {
-      __threadfence();
-      atomicAdd(gcnt, 1u);
-    }
+  // (called after a barrier that follows this CTA's exchange writes; the
+  // release orders them, through that barrier, before the count)
+  auto group_arrive = [&](unsigned st) {
+    if (tid == 0) red_release_gpu_add(gcnt + (st & 3u) * 32u, 1u);
   };
-  auto group_wait = [&](unsigned target) {
+  auto group_wait = [&](unsigned st) {
     if (tid == 0 && !s_abort) {
+      const unsigned target = (unsigned)R2 * ((st >> 2) + 1u) + a.wait_extra;
+      const unsigned* c = gcnt + (st & 3u) * 32u;
       unsigned spins = 0;
-      while (ld_acquire_gpu(gcnt) < target) {
+      while (ld_acquire_gpu(c) < target) {
         if (++spins > a.spin_limit) {
           s_abort = 1;
           *a.timeout = 1;
@@ -370,9 +391,8 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
         }
         __nanosleep(64);
       }
-      __threadfence();
     }
-    __syncthreads();  // the other CTAs' exchange writes are visible
+    __syncthreads();  // after thread 0's acquire: the other CTAs' exchange writes are visible
   };
 
   unsigned step = 0;  // inner indices processed by this CTA (selects the exchange slots)
@@ -388,7 +408,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
   {
     const CodeT* gA = reinterpret_cast<const CodeT*>(a.codeA) + ((size_t)t * R2 + r2) * a.SA;
     const CodeT* gB = reinterpret_cast<const CodeT*>(a.codeB) + ((size_t)t * R2 + r2) * a.SB;
-    for (int64_t e = tid; e < a.SA + a.SB; e += kCT) {
+    for (int64_t e = tid; e < a.SA + a.SB; e += NT) {
       const uint32_t h = e < a.SA ? (uint32_t)gA[e] : (uint32_t)gB[e - a.SA];
       const uint32_t m = h & (L - 1), q1 = h >> LOGL;
       const uint32_t w = kFFT ? ((q1 * (uint32_t)r1) & (uint32_t)(R1 - 1)) : (__popc(q1 & (uint32_t)r1) & 1u);
@@ -398,11 +418,11 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
   // this thread's contiguous slot range in its segment (compact plan)
   const uint32_t* cutA = a.countA + ((size_t)t * R2 + r2) * (kCT + 1);
   const uint32_t* cutB = a.countB + ((size_t)t * R2 + r2) * (kCT + 1);
-  const int begA = (int)cutA[tid], endA = (int)cutA[tid + 1];
-  const int begB = (int)cutB[tid], endB = (int)cutB[tid + 1];
+  const int begA = (int)cutA[tid * VPT], endA = (int)cutA[(tid + 1) * VPT];
+  const int begB = (int)cutB[tid * VPT], endB = (int)cutB[(tid + 1) * VPT];
 
   // ---- accumulators for this CTA's outputs
-  // group gi = tid + 512 u (u < OUT / 8) covers sub-spectrum position
+  // group gi = tid + NT u (u < OUT / 8) covers sub-spectrum position
   // n = r2 * (L / R2) + (gi >> (logR2 - 3)) and 8 of its R2 outputs
   const int64_t bsz = (int64_t)1 << a.log2b;
   auto out_f = [&](int gi, int jj) -> int64_t {
@@ -424,7 +444,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
   float qh[OUT][QC], ql[OUT][QC];  // two-sum pairs (FP32 path)
 #pragma unroll
   for (int o = 0; o < OUT; ++o) {
-    const int gi = tid + kCT * (o >> 3);
+    const int gi = tid + NT * (o >> 3);
     const int64_t f = out_f(gi, o & 7);
     double vx = 0.0, vy = 0.0;
     if (a.accumulate) {
@@ -457,10 +477,10 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
   auto stage = [&](int64_t k) {
     const Real* rA = reinterpret_cast<const Real*>(a.matA) + (((size_t)t * a.kc + k) * R2 + r2) * a.SA;
     const Real* rB = reinterpret_cast<const Real*>(a.matB) + (((size_t)t * a.kc + k) * R2 + r2) * a.SB;
-    for (int e = tid; e < totA; e += kCT) {
+    for (int e = tid; e < totA; e += NT) {
       if (kF32) cp_async4(stA + spad<Real>(e), rA + e); else cp_async8(stA + spad<Real>(e), rA + e);
     }
-    for (int e = tid; e < totB; e += kCT) {
+    for (int e = tid; e < totB; e += NT) {
       if (kF32) cp_async4(stB + spad<Real>(e), rB + e); else cp_async8(stB + spad<Real>(e), rB + e);
     }
   };
@@ -557,7 +577,50 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
   // writes the sub-spectrum to this CTA's exchange slot xo (natural order;
   // FWHT: (x, y) pairs) and zeros to the buffer.
   auto transform = [&](C* __restrict__ xo) {
-    if (kFFT && !kF32) {
+    if (kFFT && !kF32 && NT != kCT) {
+      // L = 2048, 256 threads: 3 radix-8 DIT passes (pass 0 applies the DIF
+      // weight w_b^{n1 r1}, r1 > 0) and a radix-4 pass of two butterflies
+      // per thread that applies the post-twiddle w_M^{n r2}
+#pragma unroll
+      for (int ps = 0; ps < 3; ++ps) {
+        const int s0 = 3 * ps, half = 1 << s0;
+        const int kk2 = tid & (half - 1);
+        const int base = ((tid >> s0) << (s0 + 3)) | kk2;
+        C x[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) x[e] = buf[phys<ES>(base + e * half)];
+        if (ps == 0) {
+          if (r1 > 0) {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+              const uint32_t m = __brev((uint32_t)(base + e)) >> (32 - LOGL);
+              const uint32_t xx = ((m << a.logR2) + (uint32_t)r2) * (uint32_t)r1;  // n1 r1 < b
+              x[e] = cmul(x[e], cmul(preHi[xx >> 9], preLo[xx & 511]));
+            }
+          }
+          r8_first(x);
+        } else {
+          r8(x, ptw[(ps == 1 ? 0 : 8) + kk2]);
+        }
+#pragma unroll
+        for (int e = 0; e < 8; ++e) buf[phys<ES>(base + e * half)] = x[e];
+        __syncthreads();
+      }
+#pragma unroll
+      for (int gg = 0; gg < 2; ++gg) {
+        const int p = tid + gg * NT;  // butterfly p < 512 at half = 512: points p + 512 e
+        C x[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) x[e] = buf[phys<ES>(p + e * 512)];
+        r4(x, ptw[72 + p]);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int n = p + e * 512;
+          __stcg(xo + n, r2 > 0 ? cmul(x[e], post(n)) : x[e]);
+          buf[phys<ES>(n)] = mk((Real)0, (Real)0);
+        }
+      }
+    } else if (kFFT && !kF32) {
       // 4 radix-8 DIT passes; pass 0 (constant twiddles) applies the DIF
       // weight w_b^{n1 r1} (r1 > 0), pass 3 the post-twiddle w_M^{n r2}
 #pragma unroll
@@ -636,7 +699,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
         const int s0 = ps == 1 ? 4 : (ps == 2 ? 7 : 10), half = 1 << s0;
 #pragma unroll
         for (int gg = 0; gg < 2; ++gg) {
-          const int gi = tid + gg * kCT;
+          const int gi = tid + gg * NT;
           const int kk2 = gi & (half - 1);
           const int base = ((gi >> s0) << (s0 + 3)) | kk2;
           C x[8];
@@ -657,45 +720,90 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
         }
         if (ps < 3) __syncthreads();
       }
-    } else if (!kF32) {
-      // FP64 WHT of x and y: radix-16 + 3 radix-8 passes, natural order
-      {
-        const int base = tid * 16;
-        Real x[16], y[16];
+    } else if (!kF32 && NT != kCT) {
+      // FP64 WHT of x and y, L = 4096, 256 threads, three radix-16 passes
+      // (the stages of a WHT commute): index bits 8-11, bits 0-3, then bits
+      // 4-7, whose pass writes the exchange slot as (x, y) pairs
 #pragma unroll
-        for (int e = 0; e < 16; ++e) { x[e] = xs[phys<ES>(base + e)]; y[e] = ys[phys<ES>(base + e)]; }
-        whtr<Real, 16>(x);
-        whtr<Real, 16>(y);
+      for (int gg = 0; gg < 2; ++gg) {
+        Real* arr = gg == 0 ? xs : ys;
+        Real v[16];
 #pragma unroll
-        for (int e = 0; e < 16; ++e) { xs[phys<ES>(base + e)] = x[e]; ys[phys<ES>(base + e)] = y[e]; }
+        for (int e = 0; e < 16; ++e) v[e] = arr[phys<ES>(tid + e * 256)];
+        whtr<Real, 16>(v);
+#pragma unroll
+        for (int e = 0; e < 16; ++e) arr[phys<ES>(tid + e * 256)] = v[e];
       }
       __syncthreads();
 #pragma unroll
-      for (int ps = 1; ps <= 3; ++ps) {
-        const int s0 = ps == 1 ? 4 : (ps == 2 ? 7 : 10), half = 1 << s0;
+      for (int gg = 0; gg < 2; ++gg) {
+        Real* arr = gg == 0 ? xs : ys;
+        const int base = tid * 16;
+        Real v[16];
 #pragma unroll
-        for (int gg = 0; gg < 2; ++gg) {
-          const int gi = tid + gg * kCT;
-          const int base = ((gi >> s0) << (s0 + 3)) | (gi & (half - 1));
-          Real x[8], y[8];
+        for (int e = 0; e < 16; ++e) v[e] = arr[phys<ES>(base + e)];
+        whtr<Real, 16>(v);
 #pragma unroll
-          for (int e = 0; e < 8; ++e) { x[e] = xs[phys<ES>(base + e * half)]; y[e] = ys[phys<ES>(base + e * half)]; }
-          whtr<Real, 8>(x);
-          whtr<Real, 8>(y);
-          if (ps == 3) {
+        for (int e = 0; e < 16; ++e) arr[phys<ES>(base + e)] = v[e];
+      }
+      __syncthreads();
+      {
+        const int base = ((tid >> 4) << 8) | (tid & 15);
+        Real x[16], y[16];
 #pragma unroll
-            for (int e = 0; e < 8; ++e) {
-              const int n = base + e * half;
-              __stcg(xo + n, mk(x[e], y[e]));
-              xs[phys<ES>(n)] = (Real)0;
-              ys[phys<ES>(n)] = (Real)0;
-            }
-          } else {
+        for (int e = 0; e < 16; ++e) { x[e] = xs[phys<ES>(base + e * 16)]; y[e] = ys[phys<ES>(base + e * 16)]; }
+        whtr<Real, 16>(x);
+        whtr<Real, 16>(y);
 #pragma unroll
-            for (int e = 0; e < 8; ++e) { xs[phys<ES>(base + e * half)] = x[e]; ys[phys<ES>(base + e * half)] = y[e]; }
-          }
+        for (int e = 0; e < 16; ++e) {
+          const int n = base + e * 16;
+          __stcg(xo + n, mk(x[e], y[e]));
+          xs[phys<ES>(n)] = (Real)0;
+          ys[phys<ES>(n)] = (Real)0;
         }
-        if (ps < 3) __syncthreads();
+      }
+    } else if (!kF32) {
+      // FP64 WHT of x and y in three passes over shared memory (the stages
+      // of a WHT commute): index bits 8-12 (radix 32, one array per
+      // thread), bits 0-3, then bits 4-7, whose pass writes the exchange
+      // slot as (x, y) pairs, 256 contiguous bytes per half-warp
+      {
+        Real* arr = tid < 256 ? xs : ys;
+        const int base = tid & 255;
+        Real v[32];
+#pragma unroll
+        for (int e = 0; e < 32; ++e) v[e] = arr[phys<ES>(base + e * 256)];
+        whtr<Real, 32>(v);
+#pragma unroll
+        for (int e = 0; e < 32; ++e) arr[phys<ES>(base + e * 256)] = v[e];
+      }
+      __syncthreads();
+#pragma unroll
+      for (int gg = 0; gg < 2; ++gg) {
+        Real* arr = gg == 0 ? xs : ys;
+        const int base = tid * 16;
+        Real v[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) v[e] = arr[phys<ES>(base + e)];
+        whtr<Real, 16>(v);
+#pragma unroll
+        for (int e = 0; e < 16; ++e) arr[phys<ES>(base + e)] = v[e];
+      }
+      __syncthreads();
+      {
+        const int base = ((tid >> 4) << 8) | (tid & 15);
+        Real x[16], y[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) { x[e] = xs[phys<ES>(base + e * 16)]; y[e] = ys[phys<ES>(base + e * 16)]; }
+        whtr<Real, 16>(x);
+        whtr<Real, 16>(y);
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+          const int n = base + e * 16;
+          __stcg(xo + n, mk(x[e], y[e]));
+          xs[phys<ES>(n)] = (Real)0;
+          ys[phys<ES>(n)] = (Real)0;
+        }
       }
     } else {
       // FP32 WHT: three Hadamard-16 factors on the tensor cores + radix-2
@@ -712,7 +820,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
       __syncthreads();
 #pragma unroll
       for (int e = 0; e < 8; ++e) {
-        const int m = tid + kCT * e;
+        const int m = tid + NT * e;
         const float x0 = fx[phys<ES>(m)], x1 = fx[phys<ES>(m + 4096)];
         const float y0 = fy[phys<ES>(m)], y1 = fy[phys<ES>(m + 4096)];
         __stcg(xo + m, mk((Real)(x0 + x1), (Real)(y0 + y1)));
@@ -730,7 +838,7 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
   auto combine = [&](const C* __restrict__ xst) {
 #pragma unroll
     for (int u = 0; u < OUT / 8; ++u) {
-      const int gi = tid + kCT * u;
+      const int gi = tid + NT * u;
       const int nl = gi >> (a.logR2 - 3);
       const int half = gi & ((R2 >> 3) - 1);
       const int n = r2 * (L >> a.logR2) + nl;
@@ -788,11 +896,14 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
 
   // ---- software pipeline over the inner indices.  On entry to an
   // iteration row kk is scattered in the buffer and row kn is being staged.
-  // The group barrier of index kk is split: the arrive follows the write of
-  // the sub-spectrum, the wait precedes the combine, and the scatter of row
-  // kn runs in between.  The exchange slots are double-buffered by the
-  // parity of the step: the barrier of step i orders every CTA's reads of
-  // step i - 1 before the writes of step i + 1.
+  // Iteration i transforms row i and writes its sub-spectrum, scatters row
+  // i + 1, arrives for step i, and only then waits for step i - 1 and
+  // combines it: an iteration separates each arrival from the wait that
+  // needs it.
+  // The exchange slots rotate over four parities (step mod 4): a CTA writes
+  // the slot of step i after its wait for step i - 2, which follows every
+  // CTA's arrival at step i - 2, which follows that CTA's combine of step
+  // i - 4, the last reader of the slot.
   int64_t kk = next_k(kb);
   int64_t kn = ke;
   if (kk < ke) {
@@ -806,38 +917,51 @@ __global__ void __launch_bounds__(kCT, 1) k_sketch_cluster(ClArgs a) {
 #ifdef CMM_PHASE_CLOCKS
   long long t_ph = 0;
 #endif
+  const C* pend = nullptr;  // exchange slots of the step whose combine is pending
   while (kk < ke) {
     CL_MARK(-1);
-    C* const xst = xgr + (size_t)(step & 1) * R2 * L;
+    // the row after next, looked up now: the load's latency hides behind
+    // the transform
+    const int64_t k2 = kn < ke ? next_k(kn + 1) : ke;
+    C* const xst = xgr + (size_t)(step & 3) * R2 * L;
     transform(xst + (size_t)r2 * L);
-    group_arrive();
     CL_MARK(0);
-    int64_t k2 = ke;
     if (kn < ke) {
       cp_async_wait_all();  // this thread's copies of row kn; the barrier publishes all
-      __syncthreads();
+      __syncthreads();      // (and the transform's exchange writes are all issued)
       CL_MARK(1);
       scatter(kn);
       CL_MARK(2);
-      k2 = next_k(kn + 1);
-      if (k2 < ke) stage(k2);  // overlaps the combine and the next transform
+    } else {
+      __syncthreads();
     }
-    group_wait((unsigned)R2 * (step + 1u) + a.wait_extra);
+    // arrive after the scatter, and wait for the previous index: the
+    // readers of this step wait for it only in the next iteration.  The
+    // next row is staged after the wait (its copies would otherwise sit in
+    // front of thread 0's barrier traffic).
+    group_arrive(step);
+    if (pend) group_wait(step - 1u);
+    if (k2 < ke) stage(k2);  // overlaps the combine and the next transform
     CL_MARK(3);
-    combine(xst);
+    if (pend) combine(pend);
     CL_MARK(4);
 #ifdef CMM_PHASE_CLOCKS
     if (tid == 0) atomicAdd(&g_cl_phase[kClPhases], 1ull);
 #endif
+    pend = xst;
     ++step;
     kk = kn;
     kn = k2;
+  }
+  if (pend) {  // the item's last step
+    group_wait(step - 1u);
+    combine(pend);
   }
 
   const bool bad = s_abort != 0;  // written before the barrier that ends this item's last wait
 #pragma unroll
   for (int o = 0; o < OUT; ++o) {
-    const int gi = tid + kCT * (o >> 3);
+    const int gi = tid + NT * (o >> 3);
     const int64_t f = out_f(gi, o & 7);
     double vx = kF32 ? (double)qh[o][0] + (double)ql[o][0] : qd[o][0];
     double vy = kF32 ? (double)qh[o][QC - 1] + (double)ql[o][QC - 1] : qd[o][QC - 1];
@@ -869,10 +993,12 @@ bool cluster_phase_cycles(double* cycles, double* steps) {
 #endif
 }
 
-static int cl_logL(int variant, bool f32) { return (variant == kVariantFFT && !f32) ? 12 : 13; }
+static int cl_logL(int variant, bool f32, int nt) {
+  return ((variant == kVariantFFT && !f32) ? 12 : 13) - (nt == kCT ? 0 : 1);
+}
 
 bool sketch_cluster_applicable(int variant, bool f32, int b) {
-  const int logL = cl_logL(variant, f32);
+  const int logL = cl_logL(variant, f32, kCT);
   int log2b = 0;
   while ((1 << log2b) < b) ++log2b;
   return log2b - logL >= 3 && log2b <= 19;  // R >= 8; DIF twiddle table covers b <= 2^19
@@ -880,23 +1006,23 @@ bool sketch_cluster_applicable(int variant, bool f32, int b) {
 
 constexpr size_t kClSmemMax = 227 * 1024 - 64;  // less the kernel's static shared bytes
 
-template <int V, typename Real, typename CodeT>
+template <int V, typename Real, typename CodeT, int NT>
 static void cl_kernel_attrs(size_t smem) {
-  CMM_CUDA(cudaFuncSetAttribute(k_sketch_cluster<V, Real, CodeT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem));
+  CMM_CUDA(cudaFuncSetAttribute(k_sketch_cluster<V, Real, CodeT, NT>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 }
 
 // shared bytes of one CTA
-static size_t cl_smem(int variant, bool f32, bool u16, int R1, int log2b, int64_t SA, int64_t SB) {
-  return cl_layout(variant == kVariantFFT, f32, u16, R1, log2b, SA, SB).total;
+static size_t cl_smem(int variant, bool f32, bool u16, int logL, int R1, int log2b, int64_t SA, int64_t SB) {
+  return cl_layout(variant == kVariantFFT, f32, u16, logL, R1, log2b, SA, SB).total;
 }
 
 // cooperative launch: the group barriers need every CTA resident
-template <int V, typename Real, typename CodeT>
+template <int V, typename Real, typename CodeT, int NT>
 static void cl_launch(const ClArgs& a, dim3 grid, size_t smem, cudaStream_t s) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
-  cfg.blockDim = dim3(kCT, 1, 1);
+  cfg.blockDim = dim3(NT, 1, 1);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
@@ -904,20 +1030,28 @@ static void cl_launch(const ClArgs& a, dim3 grid, size_t smem, cudaStream_t s) {
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  CMM_CUDA(cudaLaunchKernelEx(&cfg, k_sketch_cluster<V, Real, CodeT>, a));
+  CMM_CUDA(cudaLaunchKernelEx(&cfg, k_sketch_cluster<V, Real, CodeT, NT>, a));
 }
 
 // CTAs resident on the whole device at this shared-memory size
-template <int V, typename Real, typename CodeT>
-static int cl_resident(size_t smem) {
-  cl_kernel_attrs<V, Real, CodeT>(smem);
+template <int V, typename Real, typename CodeT, int NT>
+static int cl_resident_t(size_t smem) {
+  cl_kernel_attrs<V, Real, CodeT, NT>(smem);
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sketch_cluster<V, Real, CodeT>, kCT, smem) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sketch_cluster<V, Real, CodeT, NT>, NT, smem) !=
       cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
   return per_sm * num_sms();
+}
+static int cl_resident(int variant, bool f32, int nt, size_t smem) {
+  if (variant == kVariantFFT) {
+    if (f32) return cl_resident_t<0, float, uint16_t, kCT>(smem);
+    return nt == kCT ? cl_resident_t<0, double, uint16_t, kCT>(smem) : cl_resident_t<0, double, uint16_t, kCT / 2>(smem);
+  }
+  if (f32) return cl_resident_t<1, float, uint16_t, kCT>(smem);
+  return nt == kCT ? cl_resident_t<1, double, uint16_t, kCT>(smem) : cl_resident_t<1, double, uint16_t, kCT / 2>(smem);
 }
 
 // host-mapped flag set by a group wait that ran out of spins
@@ -942,54 +1076,71 @@ bool sketch_group_timed_out() {
   return t;
 }
 
+// threads per CTA of the FP64 group kernels: CMM_GROUP_THREADS=512|256
+// overrides the default
+static int group_threads(bool f32) {
+  if (f32) return kCT;
+  static const int nt = [] {
+    const char* e = getenv("CMM_GROUP_THREADS");
+    if (e && atoi(e) == kCT / 2) return kCT / 2;
+    if (e && atoi(e) == kCT) return kCT;
+    return kCT;
+  }();
+  return nt;
+}
+
 // Chooses R2 in {16, 8} and the k-group count G from the number of groups
 // NG = resident CTAs / R2: the grid holds NG persistent groups that share
 // the R1 * d * G work items round-robin; the estimate ceil(items/NG)/G is
 // minimised (ties to R2 = 16: less scatter redundancy, fewer items).
+// 256-thread CTAs are used only when two of them fit on an SM.
 ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, int64_t est_slots) {
   ClusterPlan C;
-  C.logL = cl_logL(variant, f32);
+  C.nt = group_threads(f32);
   C.log2b = 0;
   while ((1 << C.log2b) < b) ++C.log2b;
-  const int logR = C.log2b - C.logL;
-  double best = 1e300;
-  for (int logR2 : {4, 3}) {
-    if (logR2 > logR) continue;
-    const int R2 = 1 << logR2, R1 = 1 << (logR - logR2);
-    const size_t smem = cl_smem(variant, f32, true, R1, C.log2b, est_slots, est_slots);
-    int ctas;
-    if (variant == kVariantFFT)
-      ctas = f32 ? cl_resident<0, float, uint16_t>(smem) : cl_resident<0, double, uint16_t>(smem);
-    else
-      ctas = f32 ? cl_resident<1, float, uint16_t>(smem) : cl_resident<1, double, uint16_t>(smem);
-    const int mx = ctas / R2;
-    if (mx <= 0) continue;
-    const int64_t base = (int64_t)R1 * d;
-    for (int64_t G = 1; G <= 64; ++G) {
-      if (G > 1 && G > n_inner) break;
-      if (base * G > 65535) break;
-      const int64_t items = base * G;
-      const int64_t nc = items < mx ? items : mx;
-      // per-group load in units of one (r1, t) over all k; scatter cost ~R1
-      const double load = (double)((items + nc - 1) / nc) / (double)G * (1.0 + 0.05 * R1);
-      if (load < best - 1e-9) {
-        best = load;
-        C.logR2 = logR2;
-        C.logR1 = logR - logR2;
-        C.G = (int)G;
-        C.max_clusters = (int)nc;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    C.logL = cl_logL(variant, f32, C.nt);
+    const int logR = C.log2b - C.logL;
+    double best = 1e300;
+    for (int logR2 : {4, 3}) {
+      if (logR2 > logR) continue;
+      const int R2 = 1 << logR2, R1 = 1 << (logR - logR2);
+      const size_t smem = cl_smem(variant, f32, true, C.logL, R1, C.log2b, est_slots, est_slots);
+      if (smem > kClSmemMax) continue;
+      const int ctas = cl_resident(variant, f32, C.nt, smem);
+      if (C.nt != kCT && ctas < 2 * num_sms()) continue;
+      const int mx = ctas / R2;
+      if (mx <= 0) continue;
+      const int64_t base = (int64_t)R1 * d;
+      for (int64_t G = 1; G <= 64; ++G) {
+        if (G > 1 && G > n_inner) break;
+        if (base * G > 65535) break;
+        const int64_t items = base * G;
+        const int64_t nc = items < mx ? items : mx;
+        // per-group load in units of one (r1, t) over all k; scatter cost ~R1
+        const double load = (double)((items + nc - 1) / nc) / (double)G * (1.0 + 0.05 * R1);
+        if (load < best - 1e-9) {
+          best = load;
+          C.logR2 = logR2;
+          C.logR1 = logR - logR2;
+          C.G = (int)G;
+          C.max_clusters = (int)nc;
+        }
       }
     }
+    if (best < 1e299) break;
+    if (C.nt == kCT) throw unsupported("no group configuration fits this device");
+    C.nt = kCT;  // two 256-thread CTAs do not fit an SM: one of 512
   }
-  if (best >= 1e299) throw unsupported("no group configuration fits this device");
   if (getenv("CMM_DEBUG"))
-    fprintf(stderr, "[cmm] group plan: b=%d L=%d R1=%d R2=%d G=%d groups=%d\n", b, 1 << C.logL,
-            1 << C.logR1, 1 << C.logR2, C.G, C.max_clusters);
+    fprintf(stderr, "[cmm] group plan: b=%d L=%d R1=%d R2=%d G=%d groups=%d threads=%d\n", b, 1 << C.logL,
+            1 << C.logR1, 1 << C.logR2, C.G, C.max_clusters, C.nt);
   return C;
 }
 
 bool cluster_smem_fits(int variant, bool f32, const ClusterPlan& C, const SlabPlan& P) {
-  return cl_smem(variant, f32, P.u16, 1 << C.logR1, C.log2b, P.EA, P.EB) <= kClSmemMax;
+  return cl_smem(variant, f32, P.u16, C.logL, 1 << C.logR1, C.log2b, P.EA, P.EB) <= kClSmemMax;
 }
 
 void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const SlabPlan& P,
@@ -1017,16 +1168,16 @@ void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const Sl
   a.G = C.G;
   a.accumulate = accumulate;
   const int R2 = 1 << C.logR2, R1 = 1 << C.logR1;
-  const size_t smem = cl_smem(variant, f32, P.u16, R1, C.log2b, a.SA, a.SB);
+  const size_t smem = cl_smem(variant, f32, P.u16, C.logL, R1, C.log2b, a.SA, a.SB);
   if (smem > kClSmemMax) throw unsupported("cluster sketch: residue segments too large for shared memory");
   if (sketch_group_timed_out())
     throw std::runtime_error("cluster sketch: a group barrier wait ran out in an earlier launch");
-  // exchange area: two parities of R2 sub-spectra of L elements per group;
-  // group counters: one 128-byte line each
+  // exchange area: four parities of R2 sub-spectra of L elements per group;
+  // arrival counters: four per group, one 128-byte line each
   const size_t elem = f32 ? 8 : 16;
   const int groups = C.max_clusters;
-  DevBuf xch((size_t)groups * 2 * (size_t)R2 * ((size_t)1 << C.logL) * elem, s);
-  DevBuf gsync((size_t)groups * 128, s);
+  DevBuf xch((size_t)groups * 4 * (size_t)R2 * ((size_t)1 << C.logL) * elem, s);
+  DevBuf gsync((size_t)groups * 512, s);
   CMM_CUDA(cudaMemsetAsync(gsync.ptr, 0, gsync.bytes, s));
   a.xch = xch.ptr;
   a.gsync = gsync.as<unsigned>();
@@ -1038,22 +1189,26 @@ void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const Sl
     if (a.wait_extra) a.spin_limit = 2000;
   }
   if (getenv("CMM_DEBUG"))
-    fprintf(stderr, "[cmm] group launch: smem=%zu SA=%lld SB=%lld groups=%d exchange=%zu bytes\n", smem,
-            (long long)a.SA, (long long)a.SB, groups, xch.bytes);
+    fprintf(stderr, "[cmm] group launch: smem=%zu SA=%lld SB=%lld groups=%d threads=%d exchange=%zu bytes\n",
+            smem, (long long)a.SA, (long long)a.SB, groups, C.nt, xch.bytes);
   const dim3 grid((unsigned)R2, (unsigned)groups, 1);
   ProfScope prof("sketch", s);
   count_launch();
-#define CMM_CL(V, T, CT)                   \
-  do {                                     \
-    cl_kernel_attrs<V, T, CT>(smem);       \
-    cl_launch<V, T, CT>(a, grid, smem, s); \
+#define CMM_CL(V, T, CT, NT)                   \
+  do {                                         \
+    cl_kernel_attrs<V, T, CT, NT>(smem);       \
+    cl_launch<V, T, CT, NT>(a, grid, smem, s); \
   } while (0)
+  const bool half = C.nt != kCT;
+  if (half && f32) throw std::logic_error("256-thread group kernels are FP64 only");
   if (variant == kVariantFFT) {
-    if (f32) { if (P.u16) CMM_CL(0, float, uint16_t); else CMM_CL(0, float, uint32_t); }
-    else { if (P.u16) CMM_CL(0, double, uint16_t); else CMM_CL(0, double, uint32_t); }
+    if (f32) { if (P.u16) CMM_CL(0, float, uint16_t, kCT); else CMM_CL(0, float, uint32_t, kCT); }
+    else if (half) { if (P.u16) CMM_CL(0, double, uint16_t, kCT / 2); else CMM_CL(0, double, uint32_t, kCT / 2); }
+    else { if (P.u16) CMM_CL(0, double, uint16_t, kCT); else CMM_CL(0, double, uint32_t, kCT); }
   } else {
-    if (f32) { if (P.u16) CMM_CL(1, float, uint16_t); else CMM_CL(1, float, uint32_t); }
-    else { if (P.u16) CMM_CL(1, double, uint16_t); else CMM_CL(1, double, uint32_t); }
+    if (f32) { if (P.u16) CMM_CL(1, float, uint16_t, kCT); else CMM_CL(1, float, uint32_t, kCT); }
+    else if (half) { if (P.u16) CMM_CL(1, double, uint16_t, kCT / 2); else CMM_CL(1, double, uint32_t, kCT / 2); }
+    else { if (P.u16) CMM_CL(1, double, uint16_t, kCT); else CMM_CL(1, double, uint32_t, kCT); }
   }
 #undef CMM_CL
   CMM_CUDA(cudaGetLastError());

@@ -134,6 +134,14 @@ def test_fft_mixed(gpu, oracle, b):
     check("fft", "multiply shift", AT, B, 3, b, 5, oracle, f32=True)
 
 
+@pytest.mark.parametrize("b", [1 << 16, 1 << 18])
+def test_fwht_mixed(gpu, oracle, b):
+    rng = np.random.default_rng(b + 4)
+    AT = rng.standard_normal((29, 250))
+    B = rng.standard_normal((29, 230)) * 1e-2
+    check("fwht", "multiply shift", AT, B, 3, b, 6, oracle, f32=True)
+
+
 def test_group_wait_that_runs_out_is_reported(gpu, oracle, monkeypatch):
     """A group barrier wait is bounded: with the test hook every wait needs
     one arrival more than the group makes, so each CTA gives up after a
