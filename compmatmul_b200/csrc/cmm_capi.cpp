@@ -305,7 +305,7 @@ static bool try_cluster_plan(int variant, bool f32, const Codes& codes, int64_t 
   // kernel per product at b = 2^16 on the slab kernel) and for FP32 FWHT
   // (351 against 509 ms at b = 2^18 on the tensor-core slab kernel)
   try {
-    C = plan_cluster(variant, f32, n_inner, sp.d, sp.b, 4096);
+    C = plan_cluster(variant, f32, n_inner, sp.d, sp.b, n_a, n_b);
   } catch (const unsupported&) {
     return false;
   }

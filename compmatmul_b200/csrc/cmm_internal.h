@@ -221,7 +221,7 @@ struct ClusterPlan {
   int nt = 512;  // threads per CTA: 512, or 256 (FP64, two CTAs per SM)
 };
 bool sketch_cluster_applicable(int variant, bool f32, int b);
-ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, int64_t est_slots);
+ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, int64_t n_a, int64_t n_b);
 bool cluster_smem_fits(int variant, bool f32, const ClusterPlan& C, const SlabPlan& P);
 void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const SlabPlan& P,
                            const void* dMatA, const void* dMatB, int64_t kc, const int* dScaleExp,

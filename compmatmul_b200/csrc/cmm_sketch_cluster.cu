@@ -32,8 +32,13 @@
 // FWHT, FP64 partials).
 #include <cuda_bf16.h>
 
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
+#include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <stdexcept>
 #include <cstdlib>
 
@@ -172,6 +177,7 @@ struct ClArgs {
   unsigned* gsync;    // arrival counters, 4 per group (one 128-byte line each), zero at launch
   int* timeout;       // host-mapped flag: a group wait ran out
   unsigned spin_limit, wait_extra;
+  int tc;             // FP32 FWHT: Hadamard-16 stages on the tensor cores (else CUDA-core passes)
   int64_t SA, SB, kc, k0;
   int d, log2b, logR1, logR2, G, accumulate;
 };
@@ -762,11 +768,11 @@ __global__ void __launch_bounds__(NT, kCT / NT) k_sketch_cluster(ClArgs a) {
           ys[phys<ES>(n)] = (Real)0;
         }
       }
-    } else if (!kF32) {
-      // FP64 WHT of x and y in three passes over shared memory (the stages
-      // of a WHT commute): index bits 8-12 (radix 32, one array per
-      // thread), bits 0-3, then bits 4-7, whose pass writes the exchange
-      // slot as (x, y) pairs, 256 contiguous bytes per half-warp
+    } else if (!kF32 || !a.tc) {
+      // WHT of x and y (FP64, or FP32 on CUDA cores) in three passes over
+      // shared memory (the stages of a WHT commute): index bits 8-12 (radix
+      // 32, one array per thread), bits 0-3, then bits 4-7, whose pass
+      // writes the exchange slot as (x, y) pairs, contiguous per half-warp
       {
         Real* arr = tid < 256 ? xs : ys;
         const int base = tid & 255;
@@ -1045,13 +1051,31 @@ static int cl_resident_t(size_t smem) {
   }
   return per_sm * num_sms();
 }
-static int cl_resident(int variant, bool f32, int nt, size_t smem) {
+static int cl_resident_query(int variant, bool f32, int nt, size_t smem) {
   if (variant == kVariantFFT) {
     if (f32) return cl_resident_t<0, float, uint16_t, kCT>(smem);
     return nt == kCT ? cl_resident_t<0, double, uint16_t, kCT>(smem) : cl_resident_t<0, double, uint16_t, kCT / 2>(smem);
   }
   if (f32) return cl_resident_t<1, float, uint16_t, kCT>(smem);
   return nt == kCT ? cl_resident_t<1, double, uint16_t, kCT>(smem) : cl_resident_t<1, double, uint16_t, kCT / 2>(smem);
+}
+// the same, cached per (device, variant, precision, threads, shared bytes):
+// the occupancy query costs milliseconds of host time
+static int cl_resident(int variant, bool f32, int nt, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, int, int, size_t>, int> cache;
+  int dev = 0;
+  CMM_CUDA(cudaGetDevice(&dev));
+  const auto key = std::make_tuple(dev, variant, (int)f32, nt, smem);
+  {
+    std::lock_guard<std::mutex> g(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+  }
+  const int n = cl_resident_query(variant, f32, nt, smem);
+  std::lock_guard<std::mutex> g(mu);
+  cache[key] = n;
+  return n;
 }
 
 // host-mapped flag set by a group wait that ran out of spins
@@ -1076,6 +1100,19 @@ bool sketch_group_timed_out() {
   return t;
 }
 
+// FP32 FWHT stages: CUDA-core passes (default: measured on B200 at
+// n = 16384, b = 2^18, d = 9, 237 against 412 ms of sketch kernel per
+// product for the tensor-core Hadamard-16 stages with the BF16 hi/mid/lo
+// split, whose three products per tile cost more than the adds they
+// replace) or the tensor-core stages; CMM_MIXED_WHT=tc|cuda overrides
+static bool mixed_wht_tensor_cores() {
+  static const bool tc = [] {
+    const char* e = getenv("CMM_MIXED_WHT");
+    return e && !strcmp(e, "tc");
+  }();
+  return tc;
+}
+
 // threads per CTA of the FP64 group kernels: CMM_GROUP_THREADS=512|256
 // overrides the default
 static int group_threads(bool f32) {
@@ -1094,7 +1131,7 @@ static int group_threads(bool f32) {
 // the R1 * d * G work items round-robin; the estimate ceil(items/NG)/G is
 // minimised (ties to R2 = 16: less scatter redundancy, fewer items).
 // 256-thread CTAs are used only when two of them fit on an SM.
-ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, int64_t est_slots) {
+ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, int64_t n_a, int64_t n_b) {
   ClusterPlan C;
   C.nt = group_threads(f32);
   C.log2b = 0;
@@ -1106,7 +1143,14 @@ ClusterPlan plan_cluster(int variant, bool f32, int64_t n_inner, int d, int b, i
     for (int logR2 : {4, 3}) {
       if (logR2 > logR) continue;
       const int R2 = 1 << logR2, R1 = 1 << (logR - logR2);
-      const size_t smem = cl_smem(variant, f32, true, C.logL, R1, C.log2b, est_slots, est_slots);
+      // a CTA's segment: the indices of one residue class, n / R2 on
+      // average; the estimate allows four standard deviations (the launch
+      // checks the actual sizes)
+      auto seg = [&](int64_t n) {
+        const double m = (double)n / R2;
+        return (int64_t)(m + 4.0 * std::sqrt(m) + 64.0);
+      };
+      const size_t smem = cl_smem(variant, f32, true, C.logL, R1, C.log2b, seg(n_a), seg(n_b));
       if (smem > kClSmemMax) continue;
       const int ctas = cl_resident(variant, f32, C.nt, smem);
       if (C.nt != kCT && ctas < 2 * num_sms()) continue;
@@ -1175,7 +1219,10 @@ void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const Sl
   // exchange area: four parities of R2 sub-spectra of L elements per group;
   // arrival counters: four per group, one 128-byte line each
   const size_t elem = f32 ? 8 : 16;
-  const int groups = C.max_clusters;
+  // every CTA must be resident (cooperative launch): the actual segment
+  // sizes can need more shared memory than the plan's estimate
+  const int groups = std::min(C.max_clusters, cl_resident(variant, f32, C.nt, smem) / R2);
+  if (groups < 1) throw unsupported("cluster sketch: no group of CTAs fits the device");
   DevBuf xch((size_t)groups * 4 * (size_t)R2 * ((size_t)1 << C.logL) * elem, s);
   DevBuf gsync((size_t)groups * 512, s);
   CMM_CUDA(cudaMemsetAsync(gsync.ptr, 0, gsync.bytes, s));
@@ -1184,6 +1231,7 @@ void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const Sl
   group_timeout_flag(&a.timeout);
   a.spin_limit = 1u << 24;  // over a second of 64 ns sleeps; a step takes microseconds
   a.wait_extra = 0;
+  a.tc = mixed_wht_tensor_cores() ? 1 : 0;
   if (const char* e = getenv("CMM_TEST_GROUP_WAIT_EXTRA")) {  // test hook: waits that cannot complete
     a.wait_extra = (unsigned)atoi(e);
     if (a.wait_extra) a.spin_limit = 2000;

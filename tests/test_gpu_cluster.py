@@ -155,3 +155,48 @@ def test_group_wait_that_runs_out_is_reported(gpu, oracle, monkeypatch):
         capi().compressed_product("fft", None, AT, B, 3, 1 << 16, 9)
     monkeypatch.delenv("CMM_TEST_GROUP_WAIT_EXTRA")
     check("fft", None, AT, B, 3, 1 << 16, 9, oracle)
+
+
+_ALT_FORM = r"""
+import sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+from compmatmul_b200 import capi, lib
+rng = np.random.default_rng(int(sys.argv[3]))
+AT = rng.standard_normal((29, 250))
+B = rng.standard_normal((29, 230)) * 1e-2
+if sys.argv[4] == "f32":
+    p, _ = capi.compressed_product_f32(sys.argv[5], None, AT.astype(np.float32), B.astype(np.float32), 3, 1 << 16, 6)
+else:
+    p, _ = capi.compressed_product(sys.argv[5], None, AT, B, 3, 1 << 16, 6)
+assert lib().cmm_last_sketch_kernel().decode() == "cluster"
+np.save(sys.argv[2], p)
+"""
+
+
+@pytest.mark.parametrize("env,prec,variant", [("CMM_MIXED_WHT=tc", "f32", "fwht"),
+                                              ("CMM_GROUP_THREADS=256", "f64", "fft"),
+                                              ("CMM_GROUP_THREADS=256", "f64", "fwht")])
+def test_alternative_forms(gpu, oracle, tmp_path, env, prec, variant):
+    """The forms that the dispatch does not pick by default, each in a child
+    process (the choice is read once per process): the mixed FWHT with its
+    Hadamard-16 stages on the tensor cores (BF16 hi/mid/lo), and the FP64
+    kernels with 256-thread CTAs, two per SM."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = tmp_path / "p.npy"
+    key, val = env.split("=")
+    run_env = dict(os.environ, **{key: val})
+    subprocess.run([sys.executable, "-c", _ALT_FORM, root, str(out), "6", prec, variant], env=run_env,
+                   check=True, timeout=300)
+    p = np.load(out)
+    rng = np.random.default_rng(6)
+    AT = rng.standard_normal((29, 250))
+    B = rng.standard_normal((29, 230)) * 1e-2
+    if prec == "f32":
+        AT, B = AT.astype(np.float32).astype(np.float64), B.astype(np.float32).astype(np.float64)
+    ref = oracle.compressed_product(variant, None, AT, B, 3, 1 << 16, 6)
+    tol = 2e-5 if prec == "f32" else 1e-11
+    np.testing.assert_allclose(p, ref, rtol=0, atol=tol * float(np.abs(ref).max()))
