@@ -178,6 +178,7 @@ struct ClArgs {
   int* timeout;       // host-mapped flag: a group wait ran out
   unsigned spin_limit, wait_extra;
   int tc;             // FP32 FWHT: Hadamard-16 stages on the tensor cores (else CUDA-core passes)
+  int post_full;      // FFT: the post-twiddles as one table of L entries (else two factors)
   int64_t SA, SB, kc, k0;
   int d, log2b, logR1, logR2, G, accumulate;
 };
@@ -205,7 +206,7 @@ struct ClLayout {
 };
 __host__ __device__ inline size_t cl_align16(size_t x) { return (x + 15) & ~(size_t)15; }
 __host__ __device__ inline ClLayout cl_layout(bool fft, bool f32, bool u16, int logL, int R1, int log2b,
-                                              int64_t SA, int64_t SB) {
+                                              int64_t SA, int64_t SB, bool postFull) {
   const size_t real = f32 ? 4 : 8, cpx = 2 * real;
   const size_t L = (size_t)1 << logL;
   auto plen = [](size_t n, size_t es) { return es == 4 ? n + n / 32 : n + n / 16; };
@@ -214,7 +215,7 @@ __host__ __device__ inline ClLayout cl_layout(bool fft, bool f32, bool u16, int 
   o.buf = p;
   p += fft ? plen(L, cpx) * cpx : 2 * plen(L, real) * real;
   o.post = p;
-  if (fft) p += (128 + 64) * cpx;
+  if (fft) p += (postFull ? L : 128 + 64) * cpx;
   o.pre = p;
   if (fft && R1 > 1) p += (cl_pre_hi(log2b) + 512) * cpx;
   o.ptw = p;
@@ -274,10 +275,12 @@ __global__ void __launch_bounds__(NT, kCT / NT) k_sketch_cluster(ClArgs a) {
   const double2* tw = a.tw;
 
   // ---- shared layout (cl_layout)
-  const ClLayout lay = cl_layout(kFFT, kF32, sizeof(CodeT) == 2, LOGL, R1, a.log2b, a.SA, a.SB);
+  const bool postFull = kFFT && a.post_full;  // w_M^{n r2} tabulated for every n < L
+  const ClLayout lay = cl_layout(kFFT, kF32, sizeof(CodeT) == 2, LOGL, R1, a.log2b, a.SA, a.SB, postFull);
   C* buf0 = reinterpret_cast<C*>(sm + lay.buf);        // FFT: PL complex
   Real* xs0 = reinterpret_cast<Real*>(sm + lay.buf);   // FWHT: x: PL, y: PL real
-  C* postLo = reinterpret_cast<C*>(sm + lay.post);     // FFT: w_M^{n r2} = postHi[n >> 7] postLo[n & 127]
+  C* postLo = reinterpret_cast<C*>(sm + lay.post);     // FFT: w_M^{n r2} = postLo[n] (full table) or
+                                                       //   postHi[n >> 7] postLo[n & 127]
   C* postHi = postLo + 128;
   C* preHi = reinterpret_cast<C*>(sm + lay.pre);       // FFT, R1 > 1: w_b^{x}, x = hi * 512 + lo
   C* preLo = preHi + cl_pre_hi(a.log2b);
@@ -291,11 +294,18 @@ __global__ void __launch_bounds__(NT, kCT / NT) k_sketch_cluster(ClArgs a) {
 
   // ---- tables (constant over k)
   if (kFFT) {
-    for (int e = tid; e < 128 + 64; e += NT) {
-      const uint64_t n = e < 128 ? (uint64_t)e : (uint64_t)(e - 128) << 7;
-      if (n < (uint64_t)L) {
-        const double2 w = tw[(n * (uint64_t)r2) << a.logR1];  // w_M^{n r2} = w_b^{n r2 R1}
+    if (postFull) {
+      for (int e = tid; e < L; e += NT) {
+        const double2 w = tw[((uint64_t)e * (uint64_t)r2) << a.logR1];  // w_M^{n r2} = w_b^{n r2 R1}
         postLo[e] = mk((Real)w.x, (Real)w.y);
+      }
+    } else {
+      for (int e = tid; e < 128 + 64; e += NT) {
+        const uint64_t n = e < 128 ? (uint64_t)e : (uint64_t)(e - 128) << 7;
+        if (n < (uint64_t)L) {
+          const double2 w = tw[(n * (uint64_t)r2) << a.logR1];
+          postLo[e] = mk((Real)w.x, (Real)w.y);
+        }
       }
     }
     if (R1 > 1) {
@@ -336,7 +346,7 @@ __global__ void __launch_bounds__(NT, kCT / NT) k_sketch_cluster(ClArgs a) {
       wRy[e] = (Real)w.y;
     }
   }
-  auto post = [&](int n) -> C { return cmul(postHi[n >> 7], postLo[n & 127]); };
+  auto post = [&](int n) -> C { return postFull ? postLo[n] : cmul(postHi[n >> 7], postLo[n & 127]); };
   // B fragments of H16 for the FP32 FWHT
   uint32_t hb[2][2] = {{0u, 0u}, {0u, 0u}};
   if (!kFFT && kF32) {
@@ -943,14 +953,14 @@ __global__ void __launch_bounds__(NT, kCT / NT) k_sketch_cluster(ClArgs a) {
     }
     // arrive after the scatter, and wait for the previous index: the
     // readers of this step wait for it only in the next iteration.  The
-    // next row is staged after the wait (its copies would otherwise sit in
-    // front of thread 0's barrier traffic).
+    // next row is staged after the combine, so that its copies sit in front
+    // of neither thread 0's barrier traffic nor the combine's loads.
     group_arrive(step);
     if (pend) group_wait(step - 1u);
-    if (k2 < ke) stage(k2);  // overlaps the combine and the next transform
     CL_MARK(3);
     if (pend) combine(pend);
     CL_MARK(4);
+    if (k2 < ke) stage(k2);  // overlaps the next transform
 #ifdef CMM_PHASE_CLOCKS
     if (tid == 0) atomicAdd(&g_cl_phase[kClPhases], 1ull);
 #endif
@@ -1019,8 +1029,19 @@ static void cl_kernel_attrs(size_t smem) {
 }
 
 // shared bytes of one CTA
-static size_t cl_smem(int variant, bool f32, bool u16, int logL, int R1, int log2b, int64_t SA, int64_t SB) {
-  return cl_layout(variant == kVariantFFT, f32, u16, logL, R1, log2b, SA, SB).total;
+// (FP64 FFT: the full post-twiddle table when it fits, else the factored one)
+static size_t cl_smem(int variant, bool f32, bool u16, int logL, int R1, int log2b, int64_t SA, int64_t SB,
+                      bool* post_full = nullptr) {
+  const bool fft = variant == kVariantFFT;
+  if (fft && !f32 && logL == cl_logL(variant, f32, kCT)) {  // 512-thread form: one CTA per SM
+    const size_t full = cl_layout(fft, f32, u16, logL, R1, log2b, SA, SB, true).total;
+    if (full <= kClSmemMax) {
+      if (post_full) *post_full = true;
+      return full;
+    }
+  }
+  if (post_full) *post_full = false;
+  return cl_layout(fft, f32, u16, logL, R1, log2b, SA, SB, false).total;
 }
 
 // cooperative launch: the group barriers need every CTA resident
@@ -1212,7 +1233,9 @@ void launch_sketch_cluster(int variant, bool f32, const ClusterPlan& C, const Sl
   a.G = C.G;
   a.accumulate = accumulate;
   const int R2 = 1 << C.logR2, R1 = 1 << C.logR1;
-  const size_t smem = cl_smem(variant, f32, P.u16, C.logL, R1, C.log2b, a.SA, a.SB);
+  bool post_full = false;
+  const size_t smem = cl_smem(variant, f32, P.u16, C.logL, R1, C.log2b, a.SA, a.SB, &post_full);
+  a.post_full = post_full ? 1 : 0;
   if (smem > kClSmemMax) throw unsupported("cluster sketch: residue segments too large for shared memory");
   if (sketch_group_timed_out())
     throw std::runtime_error("cluster sketch: a group barrier wait ran out in an earlier launch");
