@@ -382,9 +382,9 @@ __global__ void __launch_bounds__(NT, kCT / NT) k_sketch_cluster(ClArgs a) {
   // Counting per slot keeps the wait exact although CTAs drift apart by a
   // step: an arrival at step s + 4 follows its CTA's wait for step s + 2,
   // hence every CTA's arrival at step s.  A wait that runs out of spins
-  // sets the host-mapped flag, and this CTA skips its later waits (it still
-  // arrives) and writes NaN partials, so the launch ends in bounded time
-  // and the failure is visible.
+  // sets the host-mapped flag, and this CTA's warps skip their later waits
+  // (it still arrives) and it writes NaN partials, so the launch ends in
+  // bounded time and the failure is visible.
   unsigned* const gcnt = a.gsync + (size_t)blockIdx.y * 128;  // 4 counters, 128 bytes apart
   __shared__ int s_abort;
   if (tid == 0) s_abort = 0;
@@ -393,8 +393,12 @@ __global__ void __launch_bounds__(NT, kCT / NT) k_sketch_cluster(ClArgs a) {
   auto group_arrive = [&](unsigned st) {
     if (tid == 0) red_release_gpu_add(gcnt + (st & 3u) * 32u, 1u);
   };
+  // Each warp waits for itself (lane 0 polls with acquire, then the warp
+  // synchronises): the combine reads only the other CTAs' global writes and
+  // registers, so no CTA-wide barrier is needed, and the warps' round trips
+  // to L2 overlap instead of all 16 warps waiting for one thread.
   auto group_wait = [&](unsigned st) {
-    if (tid == 0 && !s_abort) {
+    if (lane == 0 && !*(volatile int*)&s_abort) {
       const unsigned target = (unsigned)R2 * ((st >> 2) + 1u) + a.wait_extra;
       const unsigned* c = gcnt + (st & 3u) * 32u;
       unsigned spins = 0;
@@ -408,7 +412,7 @@ __global__ void __launch_bounds__(NT, kCT / NT) k_sketch_cluster(ClArgs a) {
         __nanosleep(64);
       }
     }
-    __syncthreads();  // after thread 0's acquire: the other CTAs' exchange writes are visible
+    __syncwarp();  // after lane 0's acquire: the other CTAs' exchange writes are visible to the warp
   };
 
   unsigned step = 0;  // inner indices processed by this CTA (selects the exchange slots)
@@ -974,7 +978,8 @@ __global__ void __launch_bounds__(NT, kCT / NT) k_sketch_cluster(ClArgs a) {
     combine(pend);
   }
 
-  const bool bad = s_abort != 0;  // written before the barrier that ends this item's last wait
+  __syncthreads();  // every warp's waits of this item are done
+  const bool bad = s_abort != 0;
 #pragma unroll
   for (int o = 0; o < OUT; ++o) {
     const int gi = tid + NT * (o >> 3);
