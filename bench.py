@@ -14,8 +14,9 @@ The default single-GPU run also measures the other workloads as short legs,
 reported as extra keys of the same JSON line ("legs"): config 2 FWHT at
 n = 16384, config 1 (n = 512, FFT), config 2 at n = 4096 (both variants),
 config 3 (mixed precision, FFT and FWHT, against the FP64 path on the same
-inputs), config 4 (256 uneven products in one batch plan) and a bounded
-config 5 serving run.
+inputs), the FP32 FWHT with its Hadamard-16 stages on the tensor cores
+(tcgen05) against CUDA cores on the same rows, config 4 (256 uneven
+products in one batch plan) and a bounded config 5 serving run.
 Each leg states its steps, its clocks and its result check.
 
 --gpus N > 1 runs under torchrun, one rank per GPU, each rank an
@@ -652,6 +653,39 @@ def leg_mixed_vs_fp64(workload, variant, warm=2, steps=3, warm64=1, steps64=2):
     return mixed
 
 
+def leg_wht_rows(rows=16384, log2n=13, warm=3, steps=1000):
+    """The FWHT's Hadamard-16 stages on the tensor cores (tcgen05 MMAs on
+    BF16 hi/mid/lo splits, FP32 accumulators in tensor memory) against the
+    same batched transform on CUDA cores: rows of 2^13 FP32 values (the
+    mixed FWHT's slab length), 512 MB in and out per call (over L2).  Each
+    call is synchronous; the time includes one host round trip per call.
+    1000 calls per form keep the timed region long enough for the clock
+    samples."""
+    import torch
+    from compmatmul_b200 import device
+    g = torch.Generator(device="cuda").manual_seed(11)
+    x = torch.randn((rows, 1 << log2n), device="cuda", generator=g, dtype=torch.float32)
+    y = torch.empty_like(x)
+    out = {"rows": rows, "row_length": 1 << log2n}
+    bytes_per_call = 2 * 4 * rows * (1 << log2n)
+    peak, _ = measured_peaks()
+    results = {}
+    for method in ("cuda", "tensor"):
+        ms, clocks = time_events(lambda: device.wht_rows(x, method, out=y), warm, steps)
+        results[method] = y.clone()
+        out[method] = {"ms_per_call": ms, "clocks": clocks, "hbm_gbs": bytes_per_call / ms / 1e6,
+                       "hbm_frac": bytes_per_call / ms / 1e6 / peak}
+    # tensor work of the two Hadamard-16 stages: 3 MMAs of 128 x 16 x 16 per 128-row tile
+    tflop = 2 * 3 * 2 * 16 * (rows * (1 << log2n)) / 1e12
+    out["tensor"]["tensor_tflops"] = tflop / (out["tensor"]["ms_per_call"] * 1e-3)
+    out["tensor_vs_cuda"] = out["cuda"]["ms_per_call"] / out["tensor"]["ms_per_call"]
+    ref = results["cuda"]
+    out["max_abs_diff_tensor_vs_cuda_rel"] = float((results["tensor"] - ref).abs().max() / ref.abs().max())
+    del x, y, results, ref
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_legs(args, reps, dAT, dB, dC, L):
     """Short legs of the other configurations (single GPU, after the
     headline): every one reports its own steps, clocks and result check."""
@@ -696,6 +730,7 @@ def run_legs(args, reps, dAT, dB, dC, L):
     guard("config2_n4096", n4096)
     for v in ("fft", "fwht"):
         guard(f"config3_{v}", lambda v=v: leg_mixed_vs_fp64("config3", v))
+    guard("wht_rows_tensor_vs_cuda", leg_wht_rows)
     bargs = argparse.Namespace(**vars(args))
     bargs.batch_variant = "both"
     guard("config4", lambda: run_batch(bargs, reps, 2, 3, compare_fp64=2, e2e_steps=1))

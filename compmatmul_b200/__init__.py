@@ -40,7 +40,7 @@ EXPORTED = [
     "cmm_batch_info", "cmm_batch_config", "cmm_batch_destroy", "cmm_server_create", "cmm_server_submit",
     "cmm_server_wait", "cmm_server_stats_get", "cmm_server_destroy", "cmm_dev_decompress_entries",
     "cmm_dev_sketch_topk", "cmm_rng_seed", "cmm_rng_next", "cmm_time_millis", "cmm_hash_params",
-    "cmm_cluster_phase_cycles",
+    "cmm_cluster_phase_cycles", "cmm_dev_wht_rows_f32",
 ]
 
 
@@ -100,6 +100,7 @@ def lib():
     L.cmm_dev_matmul_f32.argtypes = [i32, i32, i64, i64, i64, dp, dp, dp, i32, i32, u64, vp]
     L.cmm_compressed_product_f32.argtypes = [i32, i32, i64, i64, i64, dp, dp, i32, i32, i32, u64, dp, vp]
     L.cmm_matmul_f32.argtypes = [i32, i32, i64, i64, i64, dp, dp, dp, i32, i32, i32, u64]
+    L.cmm_dev_wht_rows_f32.argtypes = [vp, vp, i64, i32, i32, vp]
     L.cmm_profile_enable.argtypes = [i32]
     L.cmm_profile_enable.restype = None
     L.cmm_profile_reset.restype = None

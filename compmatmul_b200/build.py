@@ -31,7 +31,8 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
 NVFLAGS += os.environ.get("CMM_EXTRA_NVFLAGS", "").split()
 
 CUDA_SOURCES = ["cmm_sketch.cu", "cmm_sketch_v1.cu", "cmm_sketch_mixed.cu", "cmm_sketch_cluster.cu",
-                "cmm_plan.cu", "cmm_recover.cu", "cmm_noalloc.cu", "cmm_probe.cu", "cmm_batch.cu", "cmm_serve.cu"]
+                "cmm_plan.cu", "cmm_recover.cu", "cmm_noalloc.cu", "cmm_probe.cu", "cmm_batch.cu", "cmm_serve.cu",
+                "cmm_wht_tc.cu"]
 HOST_SOURCES = ["cmm_hashparams.cpp", "cmm_capi.cpp", "cmm_hostcopy.cpp"]
 
 

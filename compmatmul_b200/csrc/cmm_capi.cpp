@@ -982,6 +982,10 @@ int cmm_matmul_f32(int variant, int hash_kind, int64_t n_a, int64_t n_inner, int
   });
 }
 
+int cmm_dev_wht_rows_f32(const float* x, float* y, int64_t rows, int log2n, int method, void* stream) {
+  return guarded([&] { wht_rows_f32(x, y, rows, log2n, method, (cudaStream_t)stream); });
+}
+
 int cmm_compressed_product(int variant, int hash_kind, int64_t n_a, int64_t n_inner, int64_t n_b,
                            const double* AT, const double* B, int d, int b, int has_seed,
                            uint64_t seed, double* p_out, uint64_t* seed_out) {

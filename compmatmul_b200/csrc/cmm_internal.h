@@ -267,6 +267,8 @@ void count_launch(int n = 1);
 void set_sketch_kernel(const char* name);  // recorded for cmm_last_sketch_kernel
 bool prof_set(bool on);                    // event profiling on/off; returns the previous state
 double probe_fma_tflops(bool fp64, cudaStream_t s);
+// batched FP32 natural-order WHT of rows of 2^log2n (cmm_wht_tc.cu); synchronous on s
+void wht_rows_f32(const float* x, float* y, int64_t rows, int log2n, int method, cudaStream_t s);
 struct ProfScope {
   const char* fam;
   cudaStream_t s;

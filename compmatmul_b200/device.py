@@ -110,3 +110,27 @@ def gemm(AT, B, out=None):
     Cm = out if out is not None else torch.empty((n_a, n_b), dtype=torch.float64, device=AT.device)
     check(lib().cmm_dev_gemm(n_a, q, n_b, _ptr(Cm), _ptr(AT), _ptr(B), _stream(AT)))
     return Cm
+
+
+WHT_METHODS = {"cuda": 0, "tensor": 1}
+
+
+def wht_rows(x, method="tensor", out=None):
+    """Forward natural-order Walsh-Hadamard transform of every row of a
+    contiguous 2-D float32 CUDA tensor (rows of 2^11, 2^12 or 2^13), the
+    reference's fwht_transformer::forward (transform.hpp:94-144) on FP32.
+    method "tensor": the Hadamard-16 stages as tcgen05 MMAs on BF16
+    hi/mid/lo splits; "cuda": every stage on CUDA cores.  out may be x
+    (in place).  Returns once the rows are transformed."""
+    import torch
+    if not x.is_cuda or x.dtype != torch.float32 or not x.is_contiguous() or x.dim() != 2:
+        raise ValueError("x must be a contiguous 2-D float32 CUDA tensor")
+    rows, n = x.shape
+    log2n = n.bit_length() - 1
+    if n != 1 << log2n:
+        raise ValueError("the row length must be a power of two")
+    y = out if out is not None else torch.empty_like(x)
+    if y.shape != x.shape or y.dtype != x.dtype or not y.is_contiguous():
+        raise ValueError("out must match x")
+    check(lib().cmm_dev_wht_rows_f32(_ptr(x), _ptr(y), rows, log2n, WHT_METHODS[method], _stream(x)))
+    return y

@@ -221,6 +221,18 @@ int cmm_compressed_product_f32(int variant, int hash_kind, int64_t n_a, int64_t 
 int cmm_matmul_f32(int variant, int hash_kind, int64_t n_a, int64_t n_inner, int64_t n_b,
                    double* C, const float* AT, const float* B, int d, int b, int has_seed,
                    uint64_t seed);
+/* Batched forward Walsh-Hadamard transform of FP32 rows on device memory:
+ * y[r] = H x[r] for r < rows, each row 2^log2n floats (log2n 11..13), H
+ * the unnormalised natural-order (Sylvester) matrix.  Replaces
+ * fwht_transformer::forward (transform.hpp:94-144, FXT walsh_wak in natural
+ * order; golden values tests.cpp:621-671) for FP32 rows.  method 0: every
+ * stage on CUDA cores; method 1: the two Hadamard-16 stages as tcgen05.mma
+ * on BF16 hi/mid/lo splits with FP32 accumulators in tensor memory, the
+ * rest on CUDA cores.  x == y is allowed; x and y 16-byte aligned.
+ * Synchronous on `stream`: returns once y is written, so that a tensor-core
+ * completion wait that ran out (CMM_ERR_RUNTIME) is reported. */
+int cmm_dev_wht_rows_f32(const float* x, float* y, int64_t rows, int log2n, int method,
+                         void* stream);
 
 /* ---------------------------------------------------------------------
  * Batched products (no reference twin: the reference computes one product

@@ -55,6 +55,19 @@ def test_argument_errors_before_gpu():
     assert st == 5  # CMM_ERR_UNSUPPORTED: beyond this build's limits
 
 
+def test_wht_rows_argument_errors_before_gpu():
+    import compmatmul_b200
+    L = compmatmul_b200.lib()
+    assert L.cmm_dev_wht_rows_f32(None, None, 4, 10, 1, None) == 5  # row length beyond 2^11..2^13
+    assert b"2^11, 2^12 or 2^13" in L.cmm_last_error()
+    assert L.cmm_dev_wht_rows_f32(None, None, 4, 13, 2, None) == 1  # unknown method
+    assert L.cmm_dev_wht_rows_f32(None, None, -1, 13, 1, None) == 1
+    assert L.cmm_dev_wht_rows_f32(None, None, 4, 13, 1, None) == 1  # null rows
+    assert L.cmm_dev_wht_rows_f32(8, 16, 4, 13, 0, None) == 1  # not 16-byte aligned
+    assert b"16-byte aligned" in L.cmm_last_error()
+    assert L.cmm_dev_wht_rows_f32(None, None, 0, 13, 1, None) == 0  # nothing to do
+
+
 def _bad_calls(mod):
     """(callable, expected exception) pairs mirroring compmatmul.cpp checks."""
     A = aligned_alloc((4, 4))
