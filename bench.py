@@ -7,7 +7,7 @@ decompression of all n_a x n_b entries into HBM, and device top-K recovery
 d = 9, FFT variant, K = 256 (inputs 4.3 GB > L2, so no flush is needed).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--variant fft|fwht]
-                  [--workload config2_n16384|config2_n4096|config1|config3|config4|config5]
+                  [--workload config2_n16384|config2_n4096|config1|config3|config4|config5|wht_rows]
                   [--impl reference] [--no-legs] [--inner K]
 
 The default single-GPU run also measures the other workloads as short legs,
@@ -781,6 +781,11 @@ def main():
         return
     if args.workload == "config5":
         bench_serve(args, world, rank, local)
+        return
+    if args.workload == "wht_rows":  # the FWHT-of-rows leg alone (--n rows of 2^13)
+        if rank == 0:
+            print(json.dumps({"workload": "wht_rows",
+                              **leg_wht_rows(rows=args.n or 16384, warm=args.warmup, steps=args.steps)}))
         return
     from compmatmul_b200.planted import WORKLOADS, aligned_empty, planted_problem
     w = dict(WORKLOADS[args.workload])
