@@ -4,8 +4,10 @@
  * checker that the CUDA path is compared against.  Only tests/, the smoke
  * check and bench.py's CPU-baseline leg load it; the product never does.
  *
- * Plain C99, single threaded, FP64.  Every function names the reference
- * file:line it restates.  Parity of this restatement is pinned by the
+ * Plain C99, FP64.  The independent repetitions of the compressed product
+ * and the rows of the decompression run on OpenMP threads, with every sum
+ * in the reference's order, so results do not depend on the thread count.
+ * Every function names the reference file:line it restates.  Parity of this restatement is pinned by the
  * reference's own golden vectors (tests.cpp / test.py constants, see
  * tests/test_oracle_golden.py) and by cross-checks against the reference
  * headers compiled with project shims (oracle/_ref, see oracle/Makefile).
@@ -15,7 +17,9 @@
  *   B  is n_inner x n_b row-major, C = A^T B ... i.e. C[i][j] =
  *   sum_k AT[k][i] * B[k][j], C is n_a x n_b row-major.
  */
+#define _POSIX_C_SOURCE 200809L
 #include <math.h>
+#include <pthread.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -153,9 +157,42 @@ int cmo_hash_sign(int kind, const void* fn, uint32_t key) {
 
 /* ------------------------------------------------------------ transforms */
 
+/* Twiddles of a length-n transform (n a power of two) with direction sign:
+ * w[2j], w[2j+1] = cos, sin of the long double angle sign * 2 pi j / n, for
+ * j < n/2.  Stage len of cfft reads entry j = k (n / len): its angle
+ * sign * 2 pi k / len is the same long double value bit for bit (scaling
+ * numerator and denominator by the power of two n / len commutes with
+ * rounding), so the table changes no result; it only computes each
+ * cosl / sinl once per (n, sign) instead of once per stage and k in every
+ * call.  Tables are kept for the life of the process (guarded by a mutex:
+ * ctypes callers may run on several threads). */
+static pthread_mutex_t tw_mu = PTHREAD_MUTEX_INITIALIZER;
+static double* tw_cache[2][32];
+static const double* twiddle_table(int n, int sign) {
+  int lg = 0;
+  while ((1 << lg) < n) ++lg;
+  const int si = sign > 0;
+  pthread_mutex_lock(&tw_mu);
+  if (!tw_cache[si][lg]) {
+    const int h = n / 2 > 0 ? n / 2 : 1;
+    double* w = (double*)malloc(sizeof(double) * 2 * (size_t)h);
+    for (int j = 0; j < n / 2; ++j) {
+      const long double ang = (long double)sign * 2.0L * 3.14159265358979323846264338327950288L * j / n;
+      w[2 * j] = (double)cosl(ang);
+      w[2 * j + 1] = (double)sinl(ang);
+    }
+    tw_cache[si][lg] = w;
+  }
+  const double* w = tw_cache[si][lg];
+  pthread_mutex_unlock(&tw_mu);
+  return w;
+}
+
 /* In-place iterative radix-2 complex DFT, sign -1 (forward) or +1
- * (inverse, unnormalised).  Twiddles from long double sin/cos. */
+ * (inverse, unnormalised).  Twiddles from long double sin/cos
+ * (twiddle_table). */
 static void cfft(int n, double* re, double* im, int sign) {
+  const double* tw = twiddle_table(n, sign);
   for (int i = 1, j = 0; i < n; ++i) {
     int bit = n >> 1;
     for (; j & bit; bit >>= 1) j ^= bit;
@@ -167,10 +204,12 @@ static void cfft(int n, double* re, double* im, int sign) {
   }
   for (int len = 2; len <= n; len <<= 1) {
     const int half = len >> 1;
-    for (int k = 0; k < half; ++k) {
-      const long double ang = (long double)sign * 2.0L * 3.14159265358979323846264338327950288L * k / len;
-      const double wr = (double)cosl(ang), wi = (double)sinl(ang);
-      for (int s = 0; s < n; s += len) {
+    const int step = n / len;
+    /* every butterfly of a stage is independent: blocks outer, k inner
+     * (contiguous), the same operations as any other order */
+    for (int s = 0; s < n; s += len) {
+      for (int k = 0; k < half; ++k) {
+        const double wr = tw[2 * k * step], wi = tw[2 * k * step + 1];
         const int a = s + k, c = s + k + half;
         const double xr = re[c] * wr - im[c] * wi;
         const double xi = re[c] * wi + im[c] * wr;
@@ -274,10 +313,6 @@ int cmo_compressed_product(int variant, int kind, int64_t n_a, int64_t n_inner, 
   cmo_sketch_fns S;
   sketch_fns_init(&S, kind, d, b, seed);
   const int nc = b / 2 + 1;
-  double* pa = (double*)malloc(sizeof(double) * b);
-  double* pb = (double*)malloc(sizeof(double) * b);
-  double* Xa = (double*)malloc(sizeof(double) * 2 * nc);
-  double* Xb = (double*)malloc(sizeof(double) * 2 * nc);
   double* acc = (double*)calloc((size_t)d * (variant == CMO_FFT ? 2 * nc : b), sizeof(double));
   /* per-index codes: hash once per (t,i) instead of per (k,t,i); same values */
   uint32_t* hA = (uint32_t*)malloc(sizeof(uint32_t) * d * n_a);
@@ -294,10 +329,19 @@ int cmo_compressed_product(int variant, int kind, int64_t n_a, int64_t n_inner, 
       sB[t * n_b + j] = (int8_t)cmo_hash_sign(kind, S.s2 + S.fb * t, (uint32_t)j);
     }
   }
-  for (int64_t k = 0; k < n_inner; ++k) {
-    const double* a = AT + (size_t)k * n_a;
-    const double* bb = B + (size_t)k * n_b;
-    for (int t = 0; t < d; ++t) {
+  /* The repetitions are independent and each accumulates over k in
+   * ascending order, as the reference's k loop does for every t, so they
+   * run on separate threads (OpenMP when built with it) with the same sums
+   * in the same order: results do not depend on the thread count. */
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int t = 0; t < d; ++t) {
+    double* pa = (double*)malloc(sizeof(double) * b);
+    double* pb = (double*)malloc(sizeof(double) * b);
+    double* Xa = (double*)malloc(sizeof(double) * 2 * nc);
+    double* Xb = (double*)malloc(sizeof(double) * 2 * nc);
+    for (int64_t k = 0; k < n_inner; ++k) {
+      const double* a = AT + (size_t)k * n_a;
+      const double* bb = B + (size_t)k * n_b;
       memset(pa, 0, sizeof(double) * b);
       memset(pb, 0, sizeof(double) * b);
       /* matmul_fft.hpp:78-80 */
@@ -323,6 +367,7 @@ int cmo_compressed_product(int variant, int kind, int64_t n_a, int64_t n_inner, 
         for (int f = 0; f < b; ++f) P[f] += pa[f] * pb[f];
       }
     }
+    free(pa); free(pb); free(Xa); free(Xb);
   }
   const double inv_b = 1.0 / b;
   for (int t = 0; t < d; ++t) {
@@ -337,7 +382,7 @@ int cmo_compressed_product(int variant, int kind, int64_t n_a, int64_t n_inner, 
     }
     for (int h = 0; h < b; ++h) pt[h] *= inv_b;
   }
-  free(pa); free(pb); free(Xa); free(Xb); free(acc);
+  free(acc);
   free(hA); free(sA); free(hB); free(sB);
   sketch_fns_free(&S);
   return 0;
@@ -367,7 +412,6 @@ int cmo_decompress_rows(int variant, int kind, int d, int b, uint64_t seed, cons
   cmo_sketch_fns S;
   sketch_fns_init(&S, kind, d, b, seed);
   const uint32_t mask = (uint32_t)b - 1u;
-  double* scratch = (double*)malloc(sizeof(double) * d);
   uint32_t* h2 = (uint32_t*)malloc(sizeof(uint32_t) * d * n_b);
   int8_t* s2 = (int8_t*)malloc((size_t)d * n_b);
   for (int t = 0; t < d; ++t)
@@ -375,24 +419,32 @@ int cmo_decompress_rows(int variant, int kind, int d, int b, uint64_t seed, cons
       h2[t * n_b + j] = cmo_hash_bucket(kind, S.h2 + S.fb * t, b, (uint32_t)j);
       s2[t * n_b + j] = (int8_t)cmo_hash_sign(kind, S.s2 + S.fb * t, (uint32_t)j);
     }
-  uint32_t* h1 = (uint32_t*)malloc(sizeof(uint32_t) * d);
-  int* s1 = (int*)malloc(sizeof(int) * d);
-  for (int64_t i = i0; i < i1; ++i) {
-    for (int t = 0; t < d; ++t) {
-      h1[t] = cmo_hash_bucket(kind, S.h1 + S.fb * t, b, (uint32_t)i);
-      s1[t] = cmo_hash_sign(kind, S.s1 + S.fb * t, (uint32_t)i);
-    }
-    for (int64_t j = 0; j < n_b; ++j) {
+  /* rows are independent (each entry is its own median): OpenMP threads
+   * when built with it, each with its own scratch; the same values */
+#pragma omp parallel
+  {
+    double* scratch = (double*)malloc(sizeof(double) * d);
+    uint32_t* h1 = (uint32_t*)malloc(sizeof(uint32_t) * d);
+    int* s1 = (int*)malloc(sizeof(int) * d);
+#pragma omp for schedule(static)
+    for (int64_t i = i0; i < i1; ++i) {
       for (int t = 0; t < d; ++t) {
-        const uint32_t hj = h2[t * n_b + j];
-        const uint32_t h = variant == CMO_FFT ? ((h1[t] + hj) & mask) : (h1[t] ^ hj);
-        const int s = s1[t] * s2[t * n_b + j];
-        scratch[t] = s * p[(size_t)t * b + h];
+        h1[t] = cmo_hash_bucket(kind, S.h1 + S.fb * t, b, (uint32_t)i);
+        s1[t] = cmo_hash_sign(kind, S.s1 + S.fb * t, (uint32_t)i);
       }
-      C[(size_t)i * n_b + j] = cmo_median(d, scratch);
+      for (int64_t j = 0; j < n_b; ++j) {
+        for (int t = 0; t < d; ++t) {
+          const uint32_t hj = h2[t * n_b + j];
+          const uint32_t h = variant == CMO_FFT ? ((h1[t] + hj) & mask) : (h1[t] ^ hj);
+          const int s = s1[t] * s2[t * n_b + j];
+          scratch[t] = s * p[(size_t)t * b + h];
+        }
+        C[(size_t)i * n_b + j] = cmo_median(d, scratch);
+      }
     }
+    free(scratch); free(h1); free(s1);
   }
-  free(scratch); free(h2); free(s2); free(h1); free(s1);
+  free(h2); free(s2);
   sketch_fns_free(&S);
   return 0;
 }
