@@ -1,10 +1,14 @@
 """Pins the CPU oracle (oracle/cmm_oracle.c) against the reference's own
 golden vectors (tests.cpp, test.py) and, where oracle/_ref was built,
 against the reference's headers compiled with the project shims."""
+import os
+
 import numpy as np
 import pytest
 
 from golden import ref_vectors as G
+
+HERE = os.path.dirname(os.path.abspath(__file__))
 
 MS, MAS, TAB8, TAB16 = 0, 1, 2, 3
 
@@ -205,3 +209,42 @@ def test_oracle_matches_reference_sketch(oracle, reflib, variant, h):
     cr = np.zeros((24, 31))
     reflib.decompress_rows(variant, h, pr, 5, 64, 4242, 31, 0, 24, cr)
     assert np.array_equal(co, cr)
+
+
+_ONE_THREAD = r"""
+import sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+from oracle.oracle import Oracle
+o = Oracle()
+rng = np.random.default_rng(12)
+out = []
+for variant in ("fft", "fwht"):
+    AT = rng.standard_normal((9, 70)); B = rng.standard_normal((9, 50))
+    p = o.compressed_product(variant, "tabulation8", AT, B, 7, 1 << 12, 31)
+    out += [p, o.decompress(variant, "tabulation8", p, 7, 1 << 12, 31, 70, 50)]
+np.savez(sys.argv[2], *out)
+"""
+
+
+def test_oracle_results_independent_of_thread_count(oracle, tmp_path):
+    """The oracle runs its repetitions and decompression rows on OpenMP
+    threads with every sum in the reference's order: one thread and many
+    give bit-identical sketches and dense estimates."""
+    import subprocess
+    import sys
+    root = os.path.dirname(HERE)
+    out = str(tmp_path / "one.npz")
+    env = dict(os.environ, OMP_NUM_THREADS="1")
+    subprocess.run([sys.executable, "-c", _ONE_THREAD, root, out], env=env, check=True, timeout=300)
+    one = np.load(out)
+    rng = np.random.default_rng(12)
+    k = 0
+    for variant in ("fft", "fwht"):
+        AT = rng.standard_normal((9, 70))
+        B = rng.standard_normal((9, 50))
+        p = oracle.compressed_product(variant, "tabulation8", AT, B, 7, 1 << 12, 31)
+        C = oracle.decompress(variant, "tabulation8", p, 7, 1 << 12, 31, 70, 50)
+        assert np.array_equal(p, one[f"arr_{k}"])
+        assert np.array_equal(C, one[f"arr_{k + 1}"])
+        k += 2
