@@ -38,7 +38,6 @@
 // once more for the MMAs it issued, frees its tensor memory and returns.
 #include <cuda_bf16.h>
 
-#include <cstring>
 #include <mutex>
 
 #include "cmm_fft_device.cuh"
@@ -305,6 +304,7 @@ __global__ void __launch_bounds__(kWT) k_wht_rows(const float* x, float* y, int6
       __syncthreads();
       tc_fence_after();
     }
+    tc_fence_after();  // every warp's TMEM reads are ordered before the free (barriers above)
     if (warp == 0)
       asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kCols) : "memory");
   }
@@ -342,15 +342,22 @@ void wht_launch(const float* x, float* y, int64_t rows, int* timeout, cudaStream
   count_launch();
 }
 
+// host-mapped timeout flag of the calling host thread (one per thread, so
+// that concurrent calls from several threads do not clear each other's report)
 int* wht_timeout_flag(int** dev) {
-  static int* host = nullptr;
-  static int* mapped = nullptr;
-  static std::mutex mu;
-  std::lock_guard<std::mutex> g(mu);
+  thread_local int* host = nullptr;
+  thread_local int* mapped = nullptr;
   if (!host) {
-    CMM_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&host), sizeof(int), cudaHostAllocMapped));
-    *host = 0;
-    CMM_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&mapped), host, 0));
+    int* h = nullptr;
+    int* m = nullptr;
+    CMM_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&h), sizeof(int), cudaHostAllocMapped));
+    *h = 0;
+    if (cudaHostGetDevicePointer(reinterpret_cast<void**>(&m), h, 0) != cudaSuccess) {
+      cudaFreeHost(h);
+      throw cuda_error("cudaHostGetDevicePointer failed for the WHT timeout flag");
+    }
+    host = h;  // both set only once both calls succeeded
+    mapped = m;
   }
   if (dev) *dev = mapped;
   return host;
