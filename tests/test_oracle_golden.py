@@ -211,6 +211,25 @@ def test_oracle_matches_reference_sketch(oracle, reflib, variant, h):
     assert np.array_equal(co, cr)
 
 
+
+@pytest.mark.parametrize("variant", ["fft", "fwht"])
+@pytest.mark.parametrize("d,b", [(9, 1 << 16), (9, 1 << 18)])
+def test_oracle_matches_reference_at_config_geometry(oracle, reflib, variant, d, b):
+    """The oracle against the reference's own code at the buckets and
+    repetitions of the configurations (b = 2^16 with d = 9, and b = 2^18),
+    on a few inner indices: sketches within 1e-12 of max|p|, dense
+    decompression of the reference's sketch bit-identical."""
+    rng = np.random.default_rng(b + d)
+    AT = rng.standard_normal((6, 200))
+    B = rng.standard_normal((6, 180))
+    po = oracle.compressed_product(variant, None, AT, B, d, b, 2718)
+    pr = reflib.compressed_product(variant, None, AT, B, d, b, 2718)
+    np.testing.assert_allclose(po, pr, atol=1e-12 * np.abs(pr).max(), rtol=0)
+    co = oracle.decompress(variant, None, pr, d, b, 2718, 200, 180)
+    cr = np.zeros((200, 180))
+    reflib.decompress_rows(variant, None, pr, d, b, 2718, 180, 0, 200, cr)
+    assert np.array_equal(co, cr)
+
 _ONE_THREAD = r"""
 import sys
 import numpy as np
